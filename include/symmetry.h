@@ -1,0 +1,199 @@
+/*
+ * symmetry.h -- C ABI of the B200 lattice-update library (libsymmetry_b200.so).
+ *
+ * The reference (X-Sheen/Symmetry, Source1.f90) is one Fortran program whose
+ * time loop (Source1.f90:215-252) calls a fixed sequence of implicit-interface
+ * subroutines on FP64 arrays it owns.  This library keeps that boundary: every
+ * subroutine on the per-timestep path has an entry point of the same name,
+ * operating on device-resident state held by an opaque handle, so a Fortran
+ * driver can bind them with ISO_C_BINDING and keep its loop unchanged.
+ *
+ * Conventions
+ *   - Every function returns an int status (SYM_OK == 0) unless noted.
+ *     sym_last_error() gives a message for the last failing call on a handle.
+ *   - Host arrays use the reference's Fortran layout: scalars are
+ *     (z,y,x) column-major with z fastest; populations are (0:18,z,y,x) with
+ *     the velocity index fastest (Source1.f90:611,702,739).  The library
+ *     transposes to its own device layout on upload and back on download.
+ *   - Lattice coordinates: in SYM_MODE_REFERENCE node (x,y,z) sits at the
+ *     1-based integer position of the Fortran arrays; in SYM_MODE_CONFIG at
+ *     the 0-based position (x=0..nx-1).  Particle centres use the same frame.
+ *   - One CUDA stream per handle; calls are synchronous with respect to the
+ *     host buffers they take (the call returns after the copy completes).
+ */
+#ifndef SYMMETRY_B200_H
+#define SYMMETRY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define SYM_OK              0
+#define SYM_ERR_PARAM       1  /* invalid parameter (NaN tau, tau<=0.5, bad dims...) */
+#define SYM_ERR_OOM         2  /* device allocation failed / over budget             */
+#define SYM_ERR_CUDA        3  /* CUDA runtime error                                 */
+#define SYM_ERR_NAN         4  /* non-finite field detected                          */
+#define SYM_ERR_TIMEOUT     5  /* a bounded device wait gave up                      */
+#define SYM_ERR_STATE       6  /* call not valid in the current state                */
+#define SYM_ERR_UNSUPPORTED 7  /* feature not available for this mode/storage        */
+#define SYM_ERR_NOTFOUND    8  /* unknown field / job id                             */
+
+/* ---- geometry modes ---------------------------------------------------- */
+/* REFERENCE: the reference's own domain (Source1.f90:4, 1443-1592): updates on
+ * interior nodes 2..n-1, mirror planes at x=nx, y=1, y=ny, z=nz, halfway
+ * bounce-back wall node planes at x=1 and z=1, and every reference-geometry
+ * special case (force skip z<3/x<3 at :624, mirror force doubling :1272-1319,
+ * the pp==par/3+1 averaging :1321-1335, hard-coded repulsion planes :1607-1650,
+ * the Lagrange domain test :1832).
+ * CONFIG: periodic box (all nodes updated), optional solid wetting wall planes
+ * at x=0 and x=nx-1, minimum-image particle geometry, none of the special cases. */
+#define SYM_MODE_REFERENCE 0
+#define SYM_MODE_CONFIG    1
+
+/* ---- population storage of the fused fast path ------------------------- */
+#define SYM_STORE_FP64 0   /* plain FP64 (parity path)                                  */
+#define SYM_STORE_FP32 1   /* FP32 populations, FP32 arithmetic                         */
+#define SYM_STORE_FP16 2   /* FP16 shifted storage (deviation from w_i*rho0), FP32 math */
+
+#define SYM_MAX_PAR 32     /* particles per handle */
+
+/* Solid wall ids used in the walls/pin/pout masks for CONFIG wall planes. */
+#define SYM_WALL_ID_XLO(par) ((par) + 1)
+#define SYM_WALL_ID_XHI(par) ((par) + 2)
+
+/*
+ * Runtime replacement for the reference's compile-time constants and the
+ * hard-coded assignments in main (Source1.f90:7-26, 57-103).
+ */
+typedef struct sym_params {
+  int32_t nx, ny, nz;   /* xl, yl, zl (Source1.f90:9-11)                          */
+  int32_t mode;         /* SYM_MODE_*                                             */
+  int32_t wall_x;       /* CONFIG only: 1 = solid wetting walls at x=0 and x=nx-1 */
+  int32_t storage;      /* SYM_STORE_* used by sym_step in CONFIG mode            */
+  int32_t par;          /* number of particles, 0..SYM_MAX_PAR (:24)              */
+  int32_t la_m, la_n;   /* Lagrange grid La_m, La_n (:87-88); 0 = from alpha      */
+  int32_t reserved0;
+  double rho0;          /* reference density (:67); solid-node rho (:788)         */
+  double nu_r, nu_b;    /* kinematic viscosities of red/blue (:69-70)             */
+  /* MRT rates. A value <= 0 selects the reference's node-local rate
+   * (Source1.f90:682-684): s_e, s_eps, s_pi -> su = 1/(3nu+1/2);
+   * s_q, s_m -> sq = 8(2-su)/(8-su). */
+  double s_e, s_eps, s_q, s_pi, s_m;
+  double sigma;         /* CSF surface tension (:66, :664)                        */
+  double beta;          /* recolouring parameter (:17)                            */
+  double cita;          /* contact angle in radians (:21)                         */
+  double body[3];       /* CONFIG only: body acceleration on fluid and particles  */
+  double rad;           /* particle radius Rad (:76)                              */
+  double rho_p;         /* particle density (:79)                                 */
+  double mass;          /* particle mass (:81); <= 0 -> 4/3 rho_p pi Rad^3        */
+  double inertia;       /* moment of inertia (:82); <= 0 -> 2/5 mass Rad^2        */
+  double fg;            /* repulsion scale Fg (:84)                               */
+  double alpha;         /* Lagrange angular step (:22)                            */
+  double evap_lim;      /* EVAP_LIM (:16); <= 0 -> 1e-8                           */
+} sym_params;
+
+/* Field ids for sym_set_field / sym_get_field. Populations are double
+ * (0:18,z,y,x); scalars double (z,y,x); masks int32 (z,y,x); FLAG is int32 0/1
+ * (the storage size of a default Fortran LOGICAL). */
+enum {
+  SYM_F_RI = 0, SYM_F_BI, SYM_F_FI, SYM_F_FFI,          /* 19*N doubles */
+  SYM_F_RHO, SYM_F_UX, SYM_F_UY, SYM_F_UZ,              /* N doubles    */
+  SYM_F_RHO_N, SYM_F_RHO_R, SYM_F_RHO_B,
+  SYM_F_NX, SYM_F_NY, SYM_F_NZ, SYM_F_GRADX, SYM_F_GRADY, SYM_F_GRADZ,
+  SYM_F_FLAG,                                           /* N int32      */
+  SYM_F_WALLS, SYM_F_WALLS_OLD, SYM_F_WALLS_ALL, SYM_F_PIN, SYM_F_POUT,
+  SYM_F_COUNT
+};
+
+/* Particle state block, all (par,3) column-major like the reference
+ * (Source1.f90:46-53): index [k*par + pp] for component k of particle pp. */
+typedef struct sym_particles {
+  double center[3 * SYM_MAX_PAR];
+  double center_old[3 * SYM_MAX_PAR];
+  double center0[3 * SYM_MAX_PAR];
+  double up[3 * SYM_MAX_PAR];        /* upx, upy, upz  */
+  double rp[3 * SYM_MAX_PAR];        /* rpx, rpy, rpz  */
+  double fp[3 * SYM_MAX_PAR];        /* Fpx, Fpy, Fpz  (momentum, :1178)        */
+  double tp[3 * SYM_MAX_PAR];        /* Tpx, Tpy, Tpz                           */
+  double fre[3 * SYM_MAX_PAR];       /* Frex.. (repulsive, :1594)               */
+  double tension[3 * SYM_MAX_PAR];   /* capillary force (capillary_force2)      */
+  double tension_t[3 * SYM_MAX_PAR]; /* capillary torque                        */
+  double shb[SYM_MAX_PAR];           /* immersed area Shb (Lagrange_points)     */
+} sym_particles;
+
+typedef struct sym_handle sym_handle;
+
+/* ---- lifetime ---------------------------------------------------------- */
+/* Fill p with the reference's built-in constants (Source1.f90:9-26, 57-103)
+ * for an nx*ny*nz reference-mode domain. */
+int sym_params_reference(sym_params* p, int nx, int ny, int nz);
+/* Validate p; returns SYM_ERR_PARAM with a message in `msg` (may be NULL). */
+int sym_params_check(const sym_params* p, char* msg, size_t msg_len);
+int sym_create(const sym_params* p, int device, sym_handle** out);
+int sym_destroy(sym_handle* h);
+const char* sym_last_error(const sym_handle* h);
+/* Device bytes the handle holds (state + fast-path buffers). */
+int sym_footprint(const sym_params* p, size_t* bytes);
+
+/* ---- state transfer (Fortran layout on the host) ------------------------ */
+int sym_set_field(sym_handle* h, int field, const void* host);
+int sym_get_field(sym_handle* h, int field, void* host);
+int sym_set_particles(sym_handle* h, const sym_particles* s);
+int sym_get_particles(sym_handle* h, sym_particles* s);
+/* Lagrange point arrays (par, La_num) column-major as in :1805; any pointer may be NULL. */
+int sym_get_lagrange(sym_handle* h, double* lax, double* lay, double* laz, double* la_rhon,
+                     double* la_nx, double* la_ny, double* la_nz, int32_t* la_flag, double* ds);
+
+/* ---- initial state --------------------------------------------------------
+ * sym_initia_center     <- initia_center   Source1.f90:926-976 (REFERENCE only)
+ * sym_initialization    <- initialization  Source1.f90:850-896 (REFERENCE only)
+ * sym_init_phase        CONFIG: rho_N/rho from a host phase field, then the
+ *                       same equilibrium fill as initialization (:883-894)
+ * sym_init_thread       CONFIG: Rayleigh-Plateau thread along z, on device
+ * sym_init_slab         CONFIG: red slab z0<=z<=z1, on device                   */
+int sym_initia_center(sym_handle* h);
+int sym_initialization(sym_handle* h);
+int sym_init_phase(sym_handle* h, const double* rho_n, const double* rho);
+int sym_init_thread(sym_handle* h, double radius, double amp, double wavelength,
+                    double width, double noise, uint64_t seed);
+int sym_init_slab(sym_handle* h, double z0, double z1, double width, double noise,
+                  uint64_t seed);
+
+/* ---- the reference's per-timestep subroutines (drop-in) ------------------ */
+int sym_set_walls(sym_handle* h);         /* set_walls        Source1.f90:326-395   */
+int sym_calmacros(sym_handle* h);         /* calmacros        Source1.f90:770-831   */
+int sym_derivatives(sym_handle* h);       /* derivatives      Source1.f90:452-597   */
+int sym_collision(sym_handle* h);         /* collision+equilf Source1.f90:599-695   */
+int sym_recolor(sym_handle* h);           /* Recolor          Source1.f90:697-732   */
+int sym_boundary(sym_handle* h);          /* boundary         Source1.f90:1544-1592 */
+int sym_streaming(sym_handle* h, int which); /* streaming(ri|bi) Source1.f90:735-768; which 0=ri 1=bi */
+int sym_curve(sym_handle* h);             /* curve            Source1.f90:990-1034  */
+int sym_lagrange_points(sym_handle* h);   /* Lagrange_points  Source1.f90:1799-1978 */
+int sym_capillary_force2(sym_handle* h);  /* capillary_force2 Source1.f90:1980-2028 */
+int sym_momentum(sym_handle* h);          /* momentum         Source1.f90:1178-1261 */
+int sym_repulsive(sym_handle* h);         /* repulsive        Source1.f90:1594-1671 */
+int sym_movement(sym_handle* h);          /* movement         Source1.f90:1263-1349 */
+int sym_refilling(sym_handle* h);         /* refilling        Source1.f90:1351-1418 */
+
+/* One loop body of main (Source1.f90:216-251, output gate excluded), nsteps
+ * times.  REFERENCE mode runs the subroutine kernels above in the reference
+ * order; CONFIG mode runs the fused fast path in the handle's storage mode. */
+int sym_step(sym_handle* h, int nsteps);
+
+/* ---- diagnostics ------------------------------------------------------- */
+/* output3 (Source1.f90:1673-1717): neck height hmin on plane x=xl-1 and the y
+ * where it occurs (REFERENCE geometry). */
+int sym_output3(sym_handle* h, double* hmin, int32_t* y0);
+/* CONFIG stop rule: min over z of r_eq(z) = sqrt(sum_xy (1+phi)/2 / pi). */
+int sym_neck_radius(sym_handle* h, double* rmin);
+/* FP64 sums over fluid nodes: out[0]=sum rho_R, [1]=sum rho_B, [2..4]=momentum. */
+int sym_mass_momentum(sym_handle* h, double out[5]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SYMMETRY_B200_H */

@@ -1,0 +1,95 @@
+// state.cuh -- device state behind a sym_handle.
+#pragma once
+#include <cuda_runtime.h>
+#include <string>
+#include "../../include/symmetry.h"
+#include "lattice.cuh"
+
+namespace symb200 {
+
+// Fused fast-path state (CONFIG mode).  Populations are stored post-stream
+// (push streaming), structure of arrays [colour][velocity][node], in the
+// handle's storage type, double buffered.
+struct FastState {
+  int storage = -1;        // SYM_STORE_*
+  void* pop[2] = {nullptr, nullptr};
+  int cur = 0;             // buffer holding the current post-stream populations
+  double* phi[2] = {nullptr, nullptr};  // FP64 phase field (pin-filled), [t%2]
+  float* phif[2] = {nullptr, nullptr};  // FP32 phase field for FP32/FP16 storage
+  bool valid = false;      // fast state holds the authoritative populations
+  size_t bytes = 0;
+};
+
+}  // namespace symb200
+
+struct sym_handle {
+  sym_params p;
+  symb200::DevParams dp;
+  int device = 0;
+  cudaStream_t st = nullptr;
+  size_t N = 0;
+  // canonical state (reference arrays, SoA, FP64)
+  double *ri = nullptr, *bi = nullptr, *fi = nullptr, *ffi = nullptr, *ft = nullptr;
+  double *rho = nullptr, *ux = nullptr, *uy = nullptr, *uz = nullptr;
+  double *rhoN = nullptr, *rhoR = nullptr, *rhoB = nullptr;
+  double *nx = nullptr, *ny = nullptr, *nz = nullptr, *gx = nullptr, *gy = nullptr, *gz = nullptr;
+  int32_t *flag = nullptr, *walls = nullptr, *walls_old = nullptr, *walls_all = nullptr, *pin = nullptr,
+          *pout = nullptr;
+  // particles
+  sym_particles* dpart = nullptr;   // device copy
+  double *lax = nullptr, *lay = nullptr, *laz = nullptr, *larhon = nullptr, *lanx = nullptr, *lany = nullptr,
+         *lanz = nullptr, *lads = nullptr;
+  int32_t* laflag = nullptr;
+  double* red = nullptr;            // reduction scratch (partials)
+  size_t red_len = 0;
+  double* hred = nullptr;           // pinned host scalars
+  symb200::FastState fast;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  int graph_steps = 0;
+  size_t bytes = 0;
+  std::string err;
+};
+
+namespace symb200 {
+// launch helpers shared between translation units
+int set_error(sym_handle* h, int code, const char* fmt, ...);
+int check_cuda(sym_handle* h, cudaError_t e, const char* what);
+void fill_devparams(const sym_params& p, DevParams& d);
+
+// canonical (reference-structured) kernels, ref_kernels.cu
+int ref_calmacros(sym_handle* h);
+int ref_derivatives(sym_handle* h);
+int ref_collision(sym_handle* h);
+int ref_recolor(sym_handle* h);
+int ref_boundary(sym_handle* h);
+int ref_streaming(sym_handle* h, int which);
+int ref_curve(sym_handle* h);
+int ref_initialization(sym_handle* h);
+int ref_init_fill(sym_handle* h);    // rhoN, rho given -> populations
+int ref_init_thread(sym_handle* h, double radius, double amp, double wavelength, double width, double noise,
+                    unsigned long long seed);
+int ref_init_slab(sym_handle* h, double z0, double z1, double width, double noise, unsigned long long seed);
+int ref_neck_radius(sym_handle* h, double* rmin);
+int ref_output3(sym_handle* h, double* hmin, int32_t* y0);
+int ref_mass_momentum(sym_handle* h, double out[5]);
+int aos_to_soa(sym_handle* h, const double* dev_aos, double* dev_soa);
+int soa_to_aos(sym_handle* h, const double* dev_soa, double* dev_aos);
+
+// particle kernels, particles.cu
+int part_set_walls(sym_handle* h);
+int part_lagrange_points(sym_handle* h);
+int part_capillary_force2(sym_handle* h);
+int part_momentum(sym_handle* h);
+int part_repulsive(sym_handle* h);
+int part_movement(sym_handle* h);
+int part_refilling(sym_handle* h);
+int part_initia_center(sym_handle* h);
+
+// fused fast path, fast.cu
+int fast_alloc(sym_handle* h);
+void fast_free(sym_handle* h);
+int fast_import(sym_handle* h);   // canonical -> fast
+int fast_export(sym_handle* h);   // fast -> canonical
+int fast_step(sym_handle* h, int nsteps);
+}  // namespace symb200

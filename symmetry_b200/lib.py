@@ -1,0 +1,222 @@
+"""Python binding of libsymmetry_b200.so (the C ABI in include/symmetry.h).
+
+The Fortran reference calls its subroutines directly (Source1.f90:215-252);
+:class:`Lattice` exposes the same calls by the same names so a Python driver
+reads like the reference's ``main``.  There is no CPU fallback: importing
+this module on a machine without the built library raises, and every call
+reports CUDA errors as :class:`SymError`.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+from typing import Dict, Optional
+
+import numpy as np
+
+from .params import (FIELD_ID, INT_FIELDS, POP_FIELDS, SymParams, SymParticles)
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsymmetry_b200.so")
+HEADER = os.path.join(os.path.dirname(_HERE), "include", "symmetry.h")
+
+_lib = None
+
+
+class SymError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def header_functions(path: str = HEADER):
+    """Names of every function declared in include/symmetry.h."""
+    src = open(path).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_]*\s*\*?\s*(sym_[a-z0-9_]+)\s*\(",
+                                 src, flags=re.M)))
+
+
+def lib() -> ctypes.CDLL:
+    """Load the library; raises if it has not been built (no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run __graft_entry__.build() "
+                              "(make -C symmetry_b200/csrc)")
+        L = ctypes.CDLL(LIB_PATH)
+        H = ctypes.c_void_p
+        L.sym_create.argtypes = [ctypes.POINTER(SymParams), ctypes.c_int, ctypes.POINTER(H)]
+        L.sym_destroy.argtypes = [H]
+        L.sym_last_error.restype = ctypes.c_char_p
+        L.sym_last_error.argtypes = [H]
+        L.sym_params_reference.argtypes = [ctypes.POINTER(SymParams), ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.sym_params_check.argtypes = [ctypes.POINTER(SymParams), ctypes.c_char_p, ctypes.c_size_t]
+        L.sym_footprint.argtypes = [ctypes.POINTER(SymParams), ctypes.POINTER(ctypes.c_size_t)]
+        L.sym_set_field.argtypes = [H, ctypes.c_int, ctypes.c_void_p]
+        L.sym_get_field.argtypes = [H, ctypes.c_int, ctypes.c_void_p]
+        L.sym_set_particles.argtypes = [H, ctypes.POINTER(SymParticles)]
+        L.sym_get_particles.argtypes = [H, ctypes.POINTER(SymParticles)]
+        L.sym_get_lagrange.argtypes = [H] + [ctypes.c_void_p] * 9
+        L.sym_init_phase.argtypes = [H, ctypes.c_void_p, ctypes.c_void_p]
+        L.sym_init_thread.argtypes = [H] + [ctypes.c_double] * 5 + [ctypes.c_uint64]
+        L.sym_init_slab.argtypes = [H] + [ctypes.c_double] * 4 + [ctypes.c_uint64]
+        for n in ["initia_center", "initialization", "set_walls", "calmacros", "derivatives", "collision",
+                  "recolor", "boundary", "curve", "lagrange_points", "capillary_force2", "momentum",
+                  "repulsive", "movement", "refilling"]:
+            getattr(L, "sym_" + n).argtypes = [H]
+        L.sym_streaming.argtypes = [H, ctypes.c_int]
+        L.sym_step.argtypes = [H, ctypes.c_int]
+        L.sym_output3.argtypes = [H, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int32)]
+        L.sym_neck_radius.argtypes = [H, ctypes.POINTER(ctypes.c_double)]
+        L.sym_mass_momentum.argtypes = [H, ctypes.c_void_p]
+        _lib = L
+    return _lib
+
+
+def params_check(p: SymParams) -> Optional[str]:
+    buf = ctypes.create_string_buffer(256)
+    rc = lib().sym_params_check(ctypes.byref(p), buf, 256)
+    return None if rc == 0 else buf.value.decode()
+
+
+def footprint(p: SymParams) -> int:
+    n = ctypes.c_size_t()
+    rc = lib().sym_footprint(ctypes.byref(p), ctypes.byref(n))
+    if rc:
+        raise SymError(rc, "footprint")
+    return n.value
+
+
+class Lattice:
+    """One device-resident domain (a sym_handle)."""
+
+    def __init__(self, params: SymParams, device: int = 0):
+        self.p = params.copy()
+        self.h = ctypes.c_void_p()
+        rc = lib().sym_create(ctypes.byref(self.p), device, ctypes.byref(self.h))
+        if rc:
+            raise SymError(rc, "sym_create failed: " + (params_check(self.p) or "see stderr"))
+        self.shape = (params.nx, params.ny, params.nz)
+
+    def close(self):
+        if self.h:
+            lib().sym_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ck(self, rc: int, what: str):
+        if rc:
+            raise SymError(rc, f"{what}: {lib().sym_last_error(self.h).decode()}")
+
+    # ---- state transfer --------------------------------------------------
+    def set(self, name: str, arr: np.ndarray):
+        dt = np.int32 if name in INT_FIELDS else np.float64
+        a = np.ascontiguousarray(arr, dtype=dt)
+        want = self.p.n_nodes * (19 if name in POP_FIELDS else 1)
+        if a.size != want:
+            raise ValueError(f"{name}: expected {want} elements, got {a.size}")
+        self._ck(lib().sym_set_field(self.h, FIELD_ID[name], a.ctypes.data), f"set {name}")
+
+    def get(self, name: str) -> np.ndarray:
+        dt = np.int32 if name in INT_FIELDS else np.float64
+        shape = self.shape + ((19,) if name in POP_FIELDS else ())
+        out = np.empty(shape, dtype=dt)
+        self._ck(lib().sym_get_field(self.h, FIELD_ID[name], out.ctypes.data), f"get {name}")
+        return out
+
+    def set_particles(self, s: SymParticles):
+        self._ck(lib().sym_set_particles(self.h, ctypes.byref(s)), "set_particles")
+
+    def particles(self) -> SymParticles:
+        s = SymParticles()
+        self._ck(lib().sym_get_particles(self.h, ctypes.byref(s)), "get_particles")
+        return s
+
+    def lagrange(self) -> Dict[str, np.ndarray]:
+        n = self.la_num * self.p.par
+        names = ["Lax", "Lay", "Laz", "La_rhoN", "La_nx", "La_ny", "La_nz", "La_flag", "ds"]
+        out = {k: np.zeros(n, dtype=np.int32 if k == "La_flag" else np.float64) for k in names}
+        self._ck(lib().sym_get_lagrange(self.h, *[out[k].ctypes.data for k in names]), "get_lagrange")
+        return out
+
+    @property
+    def la_num(self) -> int:
+        if self.p.par == 0:
+            return 0
+        import math
+        lam = self.p.la_m or int(2.0 * math.pi / self.p.alpha)
+        lan = self.p.la_n or int(math.pi / self.p.alpha)
+        return lam * (lan + 1)
+
+    # ---- initial state -----------------------------------------------------
+    def initia_center(self):
+        self._ck(lib().sym_initia_center(self.h), "initia_center")
+
+    def initialization(self):
+        self._ck(lib().sym_initialization(self.h), "initialization")
+
+    def init_phase(self, phi: np.ndarray, rho: np.ndarray):
+        phi = np.ascontiguousarray(phi, dtype=np.float64)
+        rho = np.ascontiguousarray(rho, dtype=np.float64)
+        self._ck(lib().sym_init_phase(self.h, phi.ctypes.data, rho.ctypes.data), "init_phase")
+
+    def init_thread(self, radius, amp, wavelength, width=2.0, noise=1e-4, seed=0):
+        self._ck(lib().sym_init_thread(self.h, radius, amp, wavelength, width, noise, seed), "init_thread")
+
+    def init_slab(self, z0, z1, width=2.0, noise=1e-4, seed=0):
+        self._ck(lib().sym_init_slab(self.h, z0, z1, width, noise, seed), "init_slab")
+
+    # ---- the reference's subroutines -------------------------------------------
+    def call(self, name: str):
+        self._ck(getattr(lib(), "sym_" + name)(self.h), name)
+
+    def streaming(self, which: int):
+        self._ck(lib().sym_streaming(self.h, which), "streaming")
+
+    def step(self, n: int = 1):
+        self._ck(lib().sym_step(self.h, n), "step")
+
+    # ---- diagnostics -------------------------------------------------------------
+    def output3(self):
+        h, y = ctypes.c_double(), ctypes.c_int32()
+        self._ck(lib().sym_output3(self.h, ctypes.byref(h), ctypes.byref(y)), "output3")
+        return h.value, y.value
+
+    def neck_radius(self) -> float:
+        r = ctypes.c_double()
+        self._ck(lib().sym_neck_radius(self.h, ctypes.byref(r)), "neck_radius")
+        return r.value
+
+    def mass_momentum(self) -> np.ndarray:
+        out = np.zeros(5)
+        self._ck(lib().sym_mass_momentum(self.h, out.ctypes.data), "mass_momentum")
+        return out
+
+
+def setup_workload(w, device: int = 0) -> Lattice:
+    """A Lattice initialised like main (Source1.f90:208-214) for a CONFIG workload,
+    with the phase field generated on the device."""
+    from .params import particles_set
+    L = Lattice(w.params, device)
+    if w.params.par:
+        s = SymParticles()
+        particles_set(s, "center", w.params.par, [q["center"] for q in w.particles])
+        particles_set(s, "center0", w.params.par, [q["center"] for q in w.particles])
+        particles_set(s, "up", w.params.par, [q.get("up", [0, 0, 0]) for q in w.particles])
+        L.set_particles(s)
+    L.call("set_walls")
+    g = w.gen
+    if w.kind == "thread":
+        L.init_thread(g["radius"], g["amp"], g["wavelength"], g.get("width", 2.0), g.get("noise", 1e-4),
+                      g.get("seed", 0))
+    else:
+        L.init_slab(g["z0"], g["z1"], g.get("width", 2.0), g.get("noise", 1e-4), g.get("seed", 0))
+    L.call("derivatives")
+    return L

@@ -1,0 +1,168 @@
+"""GPU parity of the reference-structured kernels (one library call per
+reference subroutine) against the CPU oracle.
+
+The canonical kernels are compiled without fused multiply-add, so outside the
+transcendental calls (acos/sin/cos in the wetting rotation and the Lagrange
+points, tanh in the initial state) they round exactly like the oracle.
+Tolerances: per-subroutine 1e-12 max-relative; after many steps the field
+relative L2 error <= 1e-10, masks bit-exact, particle
+trajectories <= 1e-9.
+"""
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle, setup_reference, setup_workload as orc_setup
+from symmetry_b200 import configs, params
+from symmetry_b200.lib import Lattice, setup_workload
+from tests.common import (MASKS, SCALARS, compare_fields, compare_masks, compare_particles,
+                          copy_oracle_to_lattice, rel_l2)
+
+pytestmark = pytest.mark.gpu
+
+SEQUENCE = ["calmacros", "lagrange_points", "capillary_force2", "momentum", "repulsive", "movement",
+            "set_walls", "refilling", "derivatives", "collision", "recolor", "boundary",
+            ("streaming", 0), ("streaming", 1), "curve"]
+POPS = ["ri", "bi", "fi", "ffi"]
+
+
+def small_c2():
+    return configs.c2_wall_particle(nx=32, ny=32, nz=64, rad=5.0, centre=(16.0, 16.0, 20.0),
+                                    z0=20.0, z1=44.0, steps=300)
+
+
+def small_c1():
+    return configs.c1_thread(nx=16, ny=16, nz=48, radius=4.0)
+
+
+def cases():
+    return {
+        "c1": lambda: orc_setup(small_c1()),
+        "c2": lambda: orc_setup(small_c2()),
+        "ref": lambda: setup_reference(params.reference_params(48, 88, 48)),
+    }
+
+
+@pytest.mark.parametrize("case", ["c1", "c2", "ref"])
+def test_subroutine_parity(case):
+    o = cases()[case]()
+    L = Lattice(o.p)
+    copy_oracle_to_lattice(o, L)
+    par = o.p.par
+    for step in range(2):
+        for sub in SEQUENCE:
+            if isinstance(sub, tuple):
+                o.streaming(sub[1]); L.streaming(sub[1]); name = f"streaming{sub[1]}"
+            else:
+                if par == 0 and sub in ("lagrange_points", "capillary_force2", "momentum", "repulsive",
+                                        "movement", "refilling"):
+                    continue
+                o.call(sub); L.call(sub); name = sub
+            try:
+                compare_fields(o, L, SCALARS + POPS, 1e-12)
+                compare_masks(o, L)
+                if par:
+                    compare_particles(o, L, par, 1e-11)
+            except AssertionError as e:
+                raise AssertionError(f"{case} step {step} after {name}: {e}")
+
+
+def test_lagrange_points_parity():
+    o = setup_reference(params.reference_params(48, 88, 48))
+    L = Lattice(o.p)
+    copy_oracle_to_lattice(o, L)
+    o.call("calmacros"); L.call("calmacros")
+    o.call("lagrange_points"); L.call("lagrange_points")
+    g = L.lagrange()
+    for k in ["Lax", "Lay", "Laz", "ds", "La_rhoN", "La_nx", "La_ny", "La_nz"]:
+        a, b = g[k], o.arr(k)
+        assert np.abs(a - b).max() <= 1e-11 * max(1.0, np.abs(b).max()), k
+    assert (g["La_flag"] == o.arr("La_flag")).all()
+    s = L.particles()
+    assert np.allclose(list(s.shb)[:12], list(o.particles.shb)[:12], rtol=1e-12, atol=0)
+
+
+def _run_pair(w, steps):
+    o = orc_setup(w)
+    L = Lattice(w.params)
+    phi, rho = w.phase()
+    if w.params.par:
+        copy_oracle_to_lattice(o, L)     # identical start, particles included
+    else:
+        L.call("set_walls")
+        L.init_phase(phi, rho)
+        L.call("derivatives")
+    o.step(steps)
+    L.step(steps)
+    o.call("calmacros")
+    L.call("calmacros")
+    return o, L
+
+
+def test_c1_thread_1000_steps():
+    """Plain FP64, periodic Rayleigh-Plateau thread 32x32x96, 1000 steps."""
+    w = configs.c1_thread()
+    o, L = _run_pair(w, 1000)
+    for f in ["rho", "ux", "uy", "uz", "rho_N"]:
+        e = rel_l2(L.get(f), o.arr(f))
+        assert e <= 1e-10, (f, e)
+
+
+def test_c2_walls_particle_300_steps():
+    """Wetting walls (60 deg) + moving sphere, FP64, 32x32x64, 300 steps."""
+    w = small_c2()
+    o, L = _run_pair(w, 300)
+    fluid = o.arr("walls_all") == 0
+    for f in ["rho", "ux", "uy", "uz", "rho_N"]:
+        e = rel_l2(np.where(fluid, L.get(f), 0), np.where(fluid, o.arr(f), 0))
+        assert e <= 1e-10, (f, e)
+    compare_masks(o, L, ["walls", "walls_all", "pin", "pout"])
+    compare_particles(o, L, 1, 1e-9, ["center", "up", "rp"])
+
+
+def test_reference_mode_20_steps():
+    """The reference's own geometry (mirrors, x=1/z=1 walls, 12 particles), 48x88x48."""
+    p = params.reference_params(48, 88, 48)
+    o = setup_reference(p)
+    L = Lattice(p)
+    L.initia_center()
+    L.call("set_walls")
+    L.initialization()
+    L.call("derivatives")
+    compare_masks(o, L)
+    compare_particles(o, L, 12, 1e-13, ["center", "center0"])
+    compare_fields(o, L, ["rho_N", "rho", "ri", "bi"], 1e-13)
+    o.step(20)
+    L.step(20)
+    for f in ["rho", "ux", "uy", "uz", "rho_N"]:
+        e = rel_l2(L.get(f), o.arr(f))
+        assert e <= 1e-10, (f, e)
+    compare_masks(o, L, ["walls", "walls_all", "pin", "pout"])
+    compare_particles(o, L, 12, 1e-9, ["center", "up", "rp"])
+    h1, y1 = L.output3()
+    h2, y2 = o.output3()
+    assert y1 == y2 and abs(h1 - h2) <= 1e-9 * abs(h2)
+
+
+def test_device_init_thread_matches_host_generator():
+    w = configs.c1_thread()
+    L = setup_workload(w)
+    phi, rho = w.phase()
+    assert np.abs(L.get("rho_N") - phi).max() <= 1e-13
+    assert np.abs(L.get("rho") - rho).max() <= 1e-13
+    o = orc_setup(w)
+    compare_fields(o, L, ["ri", "bi"], 1e-13)
+
+
+def test_mass_conservation_and_diagnostics():
+    w = configs.c1_thread()
+    L = setup_workload(w)
+    m0 = L.mass_momentum()
+    L.step(200)
+    m1 = L.mass_momentum()
+    assert abs(m1[0] - m0[0]) <= 1e-12 * m0[0]
+    assert abs(m1[1] - m0[1]) <= 1e-12 * m0[1]
+    L.call("calmacros")
+    o = orc_setup(w)
+    o.step(200)
+    o.call("calmacros")
+    assert abs(L.neck_radius() - o.neck_radius()) <= 1e-10
