@@ -136,12 +136,20 @@ int sym_params_check(const sym_params* p, char* msg, size_t msg_len);
 int sym_create(const sym_params* p, int device, sym_handle** out);
 int sym_destroy(sym_handle* h);
 const char* sym_last_error(const sym_handle* h);
+/* The D3Q19 tables the kernels are compiled with: tables = cix, ciy, ciz, opc,
+ * symx, symy, symz (7 rows of 19, Source1.f90:132-138), wi (:140-142) and the
+ * moment matrix m[r*19+c] = M(r,c) of the data statement (:105-123).  Any
+ * pointer may be NULL. */
+int sym_lattice_tables(int32_t tables[7 * 19], double wi[19], double m[19 * 19]);
 /* Device bytes the handle holds (state + fast-path buffers). */
 int sym_footprint(const sym_params* p, size_t* bytes);
 
 /* ---- state transfer (Fortran layout on the host) ------------------------ */
 int sym_set_field(sym_handle* h, int field, const void* host);
 int sym_get_field(sym_handle* h, int field, void* host);
+/* Upload both colours' populations (0:18,z,y,x) in one call: the state a
+ * Fortran driver holds after initialization (Source1.f90:883-894). */
+int sym_set_populations(sym_handle* h, const double* ri, const double* bi);
 int sym_set_particles(sym_handle* h, const sym_particles* s);
 int sym_get_particles(sym_handle* h, sym_particles* s);
 /* Lagrange point arrays (par, La_num) column-major as in :1805; any pointer may be NULL. */
@@ -183,6 +191,11 @@ int sym_refilling(sym_handle* h);         /* refilling        Source1.f90:1351-1
  * times.  REFERENCE mode runs the subroutine kernels above in the reference
  * order; CONFIG mode runs the fused fast path in the handle's storage mode. */
 int sym_step(sym_handle* h, int nsteps);
+/* sym_step with CUDA events recorded on the handle's stream (CONFIG mode).
+ * use_graph=0: eager launches, ms[0]=whole region, ms[1]=phase-field kernel,
+ * ms[2]=particle coupling and pin fill, ms[3]=fused collide kernel (sums over
+ * the steps).  use_graph=1: captured-graph replay, ms[0] only (others -1). */
+int sym_step_timed(sym_handle* h, int nsteps, int use_graph, double ms[4]);
 
 /* ---- diagnostics ------------------------------------------------------- */
 /* output3 (Source1.f90:1673-1717): neck height hmin on plane x=xl-1 and the y

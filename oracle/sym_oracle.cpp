@@ -1140,6 +1140,15 @@ void orc_matrices(void* h, double* M, double* Minv) {
     for (int c = 0; c < 19; c++) { M[r * 19 + c] = o->M[r][c]; Minv[r * 19 + c] = o->Minv[r][c]; }
 }
 int orc_la_num(void* h) { return ((Orc*)h)->la_num; }
+void orc_tables(int32_t* t, double* w) {
+  for (int i = 0; i < 19; i++) {
+    t[i] = CIX[i]; t[19 + i] = CIY[i]; t[38 + i] = CIZ[i]; t[57 + i] = OPC[i];
+    t[76 + i] = SYMX[i]; t[95 + i] = SYMY[i]; t[114 + i] = SYMZ[i];
+  }
+  Orc tmp;
+  for (int i = 0; i < 19; i++) w[i] = i == 0 ? 1.0 / 3.0 : (i <= 6 ? 1.0 / 18.0 : 1.0 / 36.0);
+  (void)tmp;
+}
 
 void orc_set_walls(void* h) { set_walls(*(Orc*)h); }
 void orc_calmacros(void* h) { calmacros(*(Orc*)h); }

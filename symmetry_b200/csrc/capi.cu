@@ -307,6 +307,19 @@ int sym_destroy(sym_handle* h) {
 
 const char* sym_last_error(const sym_handle* h) { return h ? h->err.c_str() : "null handle"; }
 
+int sym_lattice_tables(int32_t tables[7 * 19], double wi[19], double m[19 * 19]) {
+  for (int i = 0; i < 19; i++) {
+    if (tables) {
+      tables[i] = CX(i); tables[19 + i] = CY(i); tables[38 + i] = CZ(i); tables[57 + i] = OPC(i);
+      tables[76 + i] = SYMX(i); tables[95 + i] = SYMY(i); tables[114 + i] = SYMZ(i);
+    }
+    if (wi) wi[i] = W(i);
+    if (m)
+      for (int c = 0; c < 19; c++) m[i * 19 + c] = MROW(i, c);
+  }
+  return SYM_OK;
+}
+
 int sym_set_field(sym_handle* h, int field, const void* host) {
   if (int e = guard(h)) return e;
   if (!host) return set_error(h, SYM_ERR_PARAM, "null host pointer");
@@ -341,6 +354,22 @@ int sym_get_field(sym_handle* h, int field, void* host) {
     return set_error(h, SYM_ERR_NOTFOUND, "unknown field %d", field);
   }
   return check_cuda(h, cudaStreamSynchronize(h->st), "get_field");
+}
+
+int sym_set_populations(sym_handle* h, const double* ri, const double* bi) {
+  if (int e = guard(h)) return e;
+  if (!ri || !bi) return set_error(h, SYM_ERR_PARAM, "null populations");
+  if (h->fast.valid) {
+    // both colours are replaced: only the fused phase field is still needed
+    if (int e = fast_export(h)) return e;
+    h->fast.valid = false;
+  }
+  const size_t N = h->N;
+  cudaMemcpyAsync(h->ft, ri, sizeof(double) * 19 * N, cudaMemcpyHostToDevice, h->st);
+  if (int e = aos_to_soa(h, h->ft, h->ri)) return e;
+  cudaMemcpyAsync(h->ft, bi, sizeof(double) * 19 * N, cudaMemcpyHostToDevice, h->st);
+  if (int e = aos_to_soa(h, h->ft, h->bi)) return e;
+  return check_cuda(h, cudaStreamSynchronize(h->st), "set_populations");
 }
 
 int sym_set_particles(sym_handle* h, const sym_particles* s) {
@@ -455,6 +484,39 @@ int sym_step(sym_handle* h, int nsteps) {
   }
   if (int e = canonical(h)) return e;
   return canonical_steps(h, nsteps);
+}
+
+int sym_step_timed(sym_handle* h, int nsteps, int use_graph, double ms[4]) {
+  if (int e = guard(h)) return e;
+  if (!ms || nsteps <= 0) return set_error(h, SYM_ERR_PARAM, "step_timed: bad arguments");
+  for (int k = 0; k < 4; k++) ms[k] = -1.0;
+  if (h->dp.ref || h->fast.storage < 0) return set_error(h, SYM_ERR_UNSUPPORTED, "step_timed: CONFIG mode only");
+  if (!h->fast.valid) {
+    if (int e = fast_import(h)) return e;
+    h->fast.valid = true;
+  }
+  if (!use_graph) return fast_step_timed(h, nsteps, ms);
+  // graph replay with events around the whole region
+  if (int e = fast_step(h, 1)) return e;   // make sure both parities are instantiated
+  if (int e = fast_step(h, 1)) return e;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  cudaEventRecord(a, h->st);
+  int rc = SYM_OK;
+  for (int t = 0; t < nsteps && !rc; t++) {
+    rc = check_cuda(h, cudaGraphLaunch(h->fast.gexec[h->fast.cur], h->st), "graph launch");
+    h->fast.cur = 1 - h->fast.cur;
+    h->fast.pc = 1 - h->fast.pc;
+  }
+  cudaEventRecord(b, h->st);
+  if (!rc) rc = check_cuda(h, cudaStreamSynchronize(h->st), "timed graph");
+  float v = 0.f;
+  if (!rc) cudaEventElapsedTime(&v, a, b);
+  ms[0] = v;
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return rc;
 }
 
 // ---- diagnostics -----------------------------------------------------------

@@ -6,6 +6,7 @@
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
+#include "../../include/symmetry.h"
 
 namespace symb200 {
 
@@ -234,13 +235,34 @@ __device__ __forceinline__ void veccross(const double a[3], const double b[3], d
 
 // Akai-2018 rotation toward the contact angle (derivatives :547-587,
 // Lagrange_points :1921-1947; the Lagrange copy has no parallel guard, :1929)
+//
+// In FP32 arithmetic (the FP32 and 16-bit storage paths) cos(theta) and
+// sin(theta) are taken as nw.n and |nw x n| (equal to the reference's
+// cos(acos(.)) and sin(acos(.)) for unit vectors) with sin(theta) held at or
+// above sin(1e-5) at both ends: in single precision nw.n rounds to exactly +-1
+// for angles up to ~3.5e-4, where the acos form divides by sin(0) = 0.
+// FP64 keeps the reference's expressions unchanged.
 template <typename R>
 __device__ __forceinline__ void akai_rotate(R cita, const R nw[3], const R n[3], bool guard, R out[3]) {
-  R theta;
   const R mx = fmax(fabs(nw[0] - n[0]), fmax(fabs(nw[1] - n[1]), fabs(nw[2] - n[2])));
-  if (guard && mx < R(1e-5)) theta = R(1e-5);
-  else theta = acos(nw[0] * n[0] + nw[1] * n[1] + nw[2] * n[2]);
-  const R sc = sin(cita), cc = cos(cita), st = sin(theta), ct = cos(theta);
+  R ct, st;
+  if (sizeof(R) == 4) {
+    if (guard && mx < R(1e-5)) {
+      ct = cos(R(1e-5));
+      st = sin(R(1e-5));
+    } else {
+      const R cx = nw[1] * n[2] - nw[2] * n[1], cy = nw[2] * n[0] - nw[0] * n[2], cz = nw[0] * n[1] - nw[1] * n[0];
+      ct = fmin(fmax(nw[0] * n[0] + nw[1] * n[1] + nw[2] * n[2], R(-1)), R(1));
+      st = fmax(sqrt(cx * cx + cy * cy + cz * cz), R(1e-5));
+    }
+  } else {
+    R theta;
+    if (guard && mx < R(1e-5)) theta = R(1e-5);
+    else theta = acos(nw[0] * n[0] + nw[1] * n[1] + nw[2] * n[2]);
+    ct = cos(theta);
+    st = sin(theta);
+  }
+  const R sc = sin(cita), cc = cos(cita);
   const R a1 = cc - sc * ct / st;
   const R a2 = cc + sc * ct / st;
   const R b1 = sc / st;
@@ -252,6 +274,21 @@ __device__ __forceinline__ void akai_rotate(R cita, const R nw[3], const R n[3],
   const R db2 = (v2[0] - n[0]) * (v2[0] - n[0]) + (v2[1] - n[1]) * (v2[1] - n[1]) + (v2[2] - n[2]) * (v2[2] - n[2]);
   if (db1 < db2) { out[0] = v1[0]; out[1] = v1[1]; out[2] = v1[2]; }
   else { out[0] = v2[0]; out[1] = v2[1]; out[2] = v2[2]; }
+}
+
+// wall normal for solid object `id` seen from node (x,y,z) (0-based indices)
+__device__ __forceinline__ void wall_normal_dev(const DevParams& P, const sym_particles* S, int id, int x, int y,
+                                                int z, double nw[3]) {
+  if (id <= P.par) {
+    const int par = P.par;
+    nw[0] = disp(P, (double)(x + P.origin), S->center[0 * par + id - 1], 0);
+    nw[1] = disp(P, (double)(y + P.origin), S->center[1 * par + id - 1], 1);
+    nw[2] = disp(P, (double)(z + P.origin), S->center[2 * par + id - 1], 2);
+    unitization(nw);
+  } else {
+    nw[0] = (id == P.par + 1) ? 1.0 : -1.0;
+    nw[1] = 0.0; nw[2] = 0.0;
+  }
 }
 
 }  // namespace symb200

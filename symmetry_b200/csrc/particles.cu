@@ -13,8 +13,6 @@ namespace symb200 {
 
 void mirror_int_all(sym_handle* h, int32_t* a, int axis);
 void mirror_macros_all(sym_handle* h);
-__device__ void wall_normal_dev(const DevParams& P, const sym_particles* S, int id, int x, int y, int z,
-                                double nw[3]);
 
 namespace {
 

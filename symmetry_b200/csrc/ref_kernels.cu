@@ -183,25 +183,6 @@ __global__ void k_gradient(DevParams P, const int32_t* __restrict__ walls_all, c
   gx[L] = g0; gy[L] = g1; gz[L] = g2; nx[L] = n0; ny[L] = n1; nz[L] = n2; flag[L] = fl;
 }
 
-}  // namespace
-
-// wall normal for solid object `id` seen from node (x,y,z) (0-based indices)
-__device__ __forceinline__ void wall_normal_dev(const DevParams& P, const sym_particles* S, int id, int x, int y,
-                                                int z, double nw[3]) {
-  if (id <= P.par) {
-    const int par = P.par;
-    nw[0] = disp(P, (double)(x + P.origin), S->center[0 * par + id - 1], 0);
-    nw[1] = disp(P, (double)(y + P.origin), S->center[1 * par + id - 1], 1);
-    nw[2] = disp(P, (double)(z + P.origin), S->center[2 * par + id - 1], 2);
-    unitization(nw);
-  } else {
-    nw[0] = (id == P.par + 1) ? 1.0 : -1.0;
-    nw[1] = 0.0; nw[2] = 0.0;
-  }
-}
-
-namespace {
-
 __global__ void k_wetting(DevParams P, const sym_particles* __restrict__ S, const int32_t* __restrict__ pout,
                           const int32_t* __restrict__ flag, double* gx, double* gy, double* gz, double* nx, double* ny,
                           double* nz) {

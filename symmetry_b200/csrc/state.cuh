@@ -14,10 +14,13 @@ struct FastState {
   int storage = -1;        // SYM_STORE_*
   void* pop[2] = {nullptr, nullptr};
   int cur = 0;             // buffer holding the current post-stream populations
-  double* phi[2] = {nullptr, nullptr};  // FP64 phase field (pin-filled), [t%2]
-  float* phif[2] = {nullptr, nullptr};  // FP32 phase field for FP32/FP16 storage
+  int pc = 0;              // phase-field buffer written by the next step
+  double* phi[2] = {nullptr, nullptr};  // FP64 halo-padded phase field (pin-filled)
+  float* phif[2] = {nullptr, nullptr};  // FP32 halo-padded phase field for FP32/FP16 storage
   bool valid = false;      // fast state holds the authoritative populations
   size_t bytes = 0;
+  cudaGraph_t graph[2] = {nullptr, nullptr};       // one captured step per buffer parity
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
 };
 
 }  // namespace symb200
@@ -92,4 +95,5 @@ void fast_free(sym_handle* h);
 int fast_import(sym_handle* h);   // canonical -> fast
 int fast_export(sym_handle* h);   // fast -> canonical
 int fast_step(sym_handle* h, int nsteps);
+int fast_step_timed(sym_handle* h, int nsteps, double ms[4]);
 }  // namespace symb200

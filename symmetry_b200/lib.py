@@ -56,6 +56,7 @@ def lib() -> ctypes.CDLL:
         L.sym_footprint.argtypes = [ctypes.POINTER(SymParams), ctypes.POINTER(ctypes.c_size_t)]
         L.sym_set_field.argtypes = [H, ctypes.c_int, ctypes.c_void_p]
         L.sym_get_field.argtypes = [H, ctypes.c_int, ctypes.c_void_p]
+        L.sym_set_populations.argtypes = [H, ctypes.c_void_p, ctypes.c_void_p]
         L.sym_set_particles.argtypes = [H, ctypes.POINTER(SymParticles)]
         L.sym_get_particles.argtypes = [H, ctypes.POINTER(SymParticles)]
         L.sym_get_lagrange.argtypes = [H] + [ctypes.c_void_p] * 9
@@ -68,6 +69,7 @@ def lib() -> ctypes.CDLL:
             getattr(L, "sym_" + n).argtypes = [H]
         L.sym_streaming.argtypes = [H, ctypes.c_int]
         L.sym_step.argtypes = [H, ctypes.c_int]
+        L.sym_step_timed.argtypes = [H, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
         L.sym_output3.argtypes = [H, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int32)]
         L.sym_neck_radius.argtypes = [H, ctypes.POINTER(ctypes.c_double)]
         L.sym_mass_momentum.argtypes = [H, ctypes.c_void_p]
@@ -131,6 +133,17 @@ class Lattice:
         self._ck(lib().sym_get_field(self.h, FIELD_ID[name], out.ctypes.data), f"get {name}")
         return out
 
+    def set_populations(self, ri: np.ndarray, bi: np.ndarray):
+        """Both colours from host arrays (pinned memory gives full PCIe rate)."""
+        for a in (ri, bi):
+            if a.dtype != np.float64 or not a.flags.c_contiguous or a.size != 19 * self.p.n_nodes:
+                raise ValueError("populations must be contiguous float64 (nx,ny,nz,19)")
+        self._ck(lib().sym_set_populations(self.h, ri.ctypes.data, bi.ctypes.data), "set_populations")
+
+    def get_into(self, name: str, out: np.ndarray):
+        """Download a field into a preallocated (e.g. pinned) host array."""
+        self._ck(lib().sym_get_field(self.h, FIELD_ID[name], out.ctypes.data), f"get {name}")
+
     def set_particles(self, s: SymParticles):
         self._ck(lib().sym_set_particles(self.h, ctypes.byref(s)), "set_particles")
 
@@ -182,6 +195,13 @@ class Lattice:
 
     def step(self, n: int = 1):
         self._ck(lib().sym_step(self.h, n), "step")
+
+    def step_timed(self, n: int, use_graph: bool = False) -> np.ndarray:
+        """Run n steps with CUDA events on the library stream; returns ms
+        [total, phase kernel, particle+pin work, collide kernel] (-1 = not timed)."""
+        ms = np.zeros(4)
+        self._ck(lib().sym_step_timed(self.h, n, 1 if use_graph else 0, ms.ctypes.data), "step_timed")
+        return ms
 
     # ---- diagnostics -------------------------------------------------------------
     def output3(self):

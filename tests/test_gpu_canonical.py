@@ -81,6 +81,20 @@ def test_lagrange_points_parity():
     assert np.allclose(list(s.shb)[:12], list(o.particles.shb)[:12], rtol=1e-12, atol=0)
 
 
+def canonical_steps(L, n):
+    """The reference loop body through the per-subroutine entry points
+    (CONFIG-mode sym_step would run the fused path instead)."""
+    for _ in range(n):
+        for sub in SEQUENCE:
+            if isinstance(sub, tuple):
+                L.streaming(sub[1])
+            elif L.p.par == 0 and sub in ("lagrange_points", "capillary_force2", "momentum", "repulsive",
+                                          "movement", "refilling"):
+                continue
+            else:
+                L.call(sub)
+
+
 def _run_pair(w, steps):
     o = orc_setup(w)
     L = Lattice(w.params)
@@ -92,7 +106,7 @@ def _run_pair(w, steps):
         L.init_phase(phi, rho)
         L.call("derivatives")
     o.step(steps)
-    L.step(steps)
+    canonical_steps(L, steps)
     o.call("calmacros")
     L.call("calmacros")
     return o, L
@@ -154,15 +168,17 @@ def test_device_init_thread_matches_host_generator():
 
 
 def test_mass_conservation_and_diagnostics():
+    """Total mass is conserved; per-colour mass matches the oracle (it is not
+    itself invariant: Recolor, Source1.f90:718-723)."""
     w = configs.c1_thread()
     L = setup_workload(w)
-    m0 = L.mass_momentum()
-    L.step(200)
-    m1 = L.mass_momentum()
-    assert abs(m1[0] - m0[0]) <= 1e-12 * m0[0]
-    assert abs(m1[1] - m0[1]) <= 1e-12 * m0[1]
-    L.call("calmacros")
     o = orc_setup(w)
+    m0 = L.mass_momentum()
+    canonical_steps(L, 200)
     o.step(200)
+    m1 = L.mass_momentum()
+    assert abs((m1[0] + m1[1]) - (m0[0] + m0[1])) <= 1e-12 * (m0[0] + m0[1])
+    assert abs(m1[0] - o.arr("ri").sum()) <= 1e-12 * m0[0]
+    L.call("calmacros")
     o.call("calmacros")
     assert abs(L.neck_radius() - o.neck_radius()) <= 1e-10
