@@ -206,6 +206,27 @@ int sym_neck_radius(sym_handle* h, double* rmin);
 /* FP64 sums over fluid nodes: out[0]=sum rho_R, [1]=sum rho_B, [2..4]=momentum. */
 int sym_mass_momentum(sym_handle* h, double out[5]);
 
+/* The same five sums for callers that may not allocate device memory: no
+ * counterpart in the reference.  It is meant for code that never creates a
+ * handle and must not call cudaMalloc -- for example a serving loop that has
+ * reserved its whole device budget up front, or a host program whose own
+ * memory manager owns every device byte -- because an allocation there can
+ * fail or stall the device.  It calls no cudaMalloc, cudaFree or allocating
+ * library routine: its scratch is a fixed 2.6 MB array inside the library
+ * (held on every GPU that loads the library until the process exits).
+ *   ri, bi     device populations, structure of arrays [19][n_nodes] (FP64)
+ *   walls_all  device int32 mask (nodes with walls_all > 0 are skipped), or NULL
+ *   n_nodes    1 .. 16,777,216; larger sizes are rejected with SYM_ERR_PARAM
+ *   out        device memory for 5 doubles, written on `stream`
+ *   stream     cudaStream_t to enqueue on (NULL = legacy default stream)
+ *   msg        optional buffer for an error message
+ * The call is asynchronous on `stream`.  The first call on each device looks
+ * up the scratch address (cudaGetSymbolAddress) and should come before any
+ * stream capture.  Calls share the scratch: calls that overlap on the GPU
+ * race, so serialise them (one stream, or events). */
+int sym_mass_momentum_noalloc(const double* ri, const double* bi, const int32_t* walls_all, int64_t n_nodes,
+                              double* out, void* stream, char* msg, size_t msg_len);
+
 #ifdef __cplusplus
 }
 #endif

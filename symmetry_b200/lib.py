@@ -73,6 +73,8 @@ def lib() -> ctypes.CDLL:
         L.sym_output3.argtypes = [H, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int32)]
         L.sym_neck_radius.argtypes = [H, ctypes.POINTER(ctypes.c_double)]
         L.sym_mass_momentum.argtypes = [H, ctypes.c_void_p]
+        L.sym_mass_momentum_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]
         _lib = L
     return _lib
 
