@@ -197,6 +197,30 @@ int sym_step(sym_handle* h, int nsteps);
  * the steps).  use_graph=1: captured-graph replay, ms[0] only (others -1). */
 int sym_step_timed(sym_handle* h, int nsteps, int use_graph, double ms[4]);
 
+/* ---- batches: many independent CONFIG domains stepped together ----------
+ * No counterpart in the reference (it runs one domain).  A batch references
+ * existing handles (same device, CONFIG mode, same storage) and steps them in
+ * lockstep: one CUDA graph per step containing one phase-field launch for all
+ * domains, the per-domain particle/wall work, and one persistent collide
+ * launch whose CTAs pull 32x8xX tiles of any domain from a work-tile table
+ * (largest first).  Results per domain are identical to sym_step on that
+ * domain alone with the same tile x extent.  Member handles stay usable on
+ * their own; the batch rebuilds its graphs when a member was stepped or read
+ * back outside it. */
+typedef struct sym_batch sym_batch;
+int sym_batch_create(sym_handle* const* handles, int n, sym_batch** out);
+int sym_batch_destroy(sym_batch* b);
+const char* sym_batch_last_error(const sym_batch* b);
+int sym_batch_step(sym_batch* b, int nsteps);
+/* nsteps graph steps bracketed by CUDA events on the batch stream; *ms = elapsed. */
+int sym_batch_step_timed(sym_batch* b, int nsteps, double* ms);
+int sym_batch_set_xchunk(sym_batch* b, int domain, int xchunk);
+int sym_batch_get_xchunk(sym_batch* b, int domain, int* xchunk);
+/* Picks the tile x extent per size class (nx <= 32, <= 48, larger) from
+ * {8,16,32,64} by timing; the trial steps advance every domain (*steps_taken). */
+int sym_batch_autotune(sym_batch* b, int trial_steps, int* steps_taken);
+int sym_batch_info(sym_batch* b, int64_t* nodes, int* ntiles, int* grid);
+
 /* ---- diagnostics ------------------------------------------------------- */
 /* output3 (Source1.f90:1673-1717): neck height hmin on plane x=xl-1 and the y
  * where it occurs (REFERENCE geometry). */

@@ -1,0 +1,435 @@
+// batch.cu -- many independent CONFIG domains stepped together.
+//
+// One step of a batch is one CUDA graph:
+//   k_phase_batch     calmacros of every domain in one launch (blocks map to
+//                     domains through a prefix sum of per-domain block counts);
+//   per-domain sparse particle coupling and pin fill (only domains with
+//                     solids; these are the small kernels of fast.cu);
+//   k_collide_batch   one persistent launch (one CTA per SM slot) whose CTAs
+//                     take 32x8xX tiles of any domain from a work-tile table
+//                     through an atomic counter, largest tiles first, so
+//                     domains of uneven size share the GPU without tails.
+// Each domain keeps its own buffers and parity; two graphs (one per parity
+// of the domain buffers) alternate.  The x extent X of the tiles is chosen per
+// size class by sym_batch_autotune.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include "state.cuh"
+#include "fused.cuh"
+
+using namespace symb200;
+using namespace symb200::fused;
+
+namespace {
+
+struct DomainDesc {
+  DevParams P;
+  Pad pd;
+  const void* pin;      // populations read this step
+  void* pnext;          // populations written this step
+  void* phic;           // phase field of this step
+  const int32_t* walls;
+  const int32_t* walls_all;
+  const int32_t* pout;
+  const sym_particles* Sp;
+  double* ffi;
+  int solid;
+  int pad_;
+};
+
+struct TileEntry {
+  int dom, z0, y0, xa, xb, cost, r0, r1;
+};
+
+constexpr int kTPB = BZ * BY;
+
+__device__ __forceinline__ int find_domain(const long long* __restrict__ off, int n, long long b) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (off[mid] <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <typename S>
+__global__ void __launch_bounds__(256) k_phase_batch(const DomainDesc* __restrict__ descs,
+                                                     const long long* __restrict__ blk_off, int ndom) {
+  using R = typename Codec<S>::R;
+  const int d = find_domain(blk_off, ndom, blockIdx.x);
+  const DomainDesc& D = descs[d];
+  const long long L = (blockIdx.x - blk_off[d]) * 256LL + threadIdx.x;
+  if (D.solid)
+    phase_node<S, true>(D.P, D.pd, (const S*)D.pin, (R*)D.phic, D.walls_all, L);
+  else
+    phase_node<S, false>(D.P, D.pd, (const S*)D.pin, (R*)D.phic, D.walls_all, L);
+}
+
+template <typename S>
+__global__ void __launch_bounds__(kTPB, 2) k_collide_batch(const DomainDesc* __restrict__ descs,
+                                                           const TileEntry* __restrict__ tiles, int ntiles,
+                                                           int* __restrict__ counter) {
+  using R = typename Codec<S>::R;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem<R>& sm = *reinterpret_cast<Smem<R>*>(smem_raw);
+  __shared__ int s_tile;
+  __shared__ __align__(16) DomainDesc s_desc;
+  for (;;) {
+    if (threadIdx.x == 0) s_tile = atomicAdd(counter, 1);
+    __syncthreads();
+    const int t = s_tile;
+    if (t >= ntiles) break;
+    const TileEntry e = tiles[t];
+    {  // stage the tile's domain descriptor in shared memory
+      const int* src = reinterpret_cast<const int*>(&descs[e.dom]);
+      int* dst = reinterpret_cast<int*>(&s_desc);
+      for (int k = threadIdx.x; k < (int)(sizeof(DomainDesc) / sizeof(int)); k += kTPB) dst[k] = src[k];
+    }
+    __syncthreads();
+    const DomainDesc& D = s_desc;
+    if (D.solid)
+      collide_tile<S, true>(D.P, D.pd, (const S*)D.pin, (S*)D.pnext, (const R*)D.phic, D.walls, D.walls_all, D.pout,
+                            D.Sp, D.ffi, e.z0, e.y0, e.xa, e.xb, sm);
+    else
+      collide_tile<S, false>(D.P, D.pd, (const S*)D.pin, (S*)D.pnext, (const R*)D.phic, D.walls, D.walls_all,
+                             D.pout, D.Sp, D.ffi, e.z0, e.y0, e.xa, e.xb, sm);
+    __syncthreads();
+  }
+}
+
+template <typename S>
+int set_batch_smem(cudaStream_t, int* grid_blocks, int device) {
+  using R = typename Codec<S>::R;
+  const int shm = (int)sizeof(Smem<R>);
+  if (cudaFuncSetAttribute(k_collide_batch<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, shm) != cudaSuccess)
+    return SYM_ERR_CUDA;
+  int per_sm = 0, sms = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_collide_batch<S>, kTPB, shm);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  *grid_blocks = std::max(1, per_sm) * std::max(1, sms);
+  return SYM_OK;
+}
+
+}  // namespace
+
+struct sym_batch {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  int storage = -1;
+  std::vector<sym_handle*> doms;
+  std::vector<int> xchunk;
+  std::vector<int> built_cur, built_pc;   // domain parities graph 0 was built for
+  int steps_since_build = 0;
+  DomainDesc* d_desc[2] = {nullptr, nullptr};
+  long long* d_blk_off = nullptr;
+  TileEntry* d_tiles = nullptr;
+  int ntiles = 0;
+  long long nblocks = 0;
+  int* d_counter = nullptr;
+  int grid = 0;
+  cudaGraph_t graph[2] = {nullptr, nullptr};
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  bool built = false;
+  std::string err;
+};
+
+namespace {
+
+int berr(sym_batch* b, int code, const char* msg) {
+  if (b) b->err = msg;
+  return code;
+}
+int bcuda(sym_batch* b, cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return SYM_OK;
+  std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+  return berr(b, e == cudaErrorMemoryAllocation ? SYM_ERR_OOM : SYM_ERR_CUDA, m.c_str());
+}
+
+void free_graphs(sym_batch* b) {
+  for (int k = 0; k < 2; k++) {
+    if (b->gexec[k]) cudaGraphExecDestroy(b->gexec[k]);
+    if (b->graph[k]) cudaGraphDestroy(b->graph[k]);
+    b->gexec[k] = nullptr;
+    b->graph[k] = nullptr;
+  }
+  b->built = false;
+}
+
+void free_tables(sym_batch* b) {
+  for (int k = 0; k < 2; k++)
+    if (b->d_desc[k]) { cudaFree(b->d_desc[k]); b->d_desc[k] = nullptr; }
+  if (b->d_blk_off) { cudaFree(b->d_blk_off); b->d_blk_off = nullptr; }
+  if (b->d_tiles) { cudaFree(b->d_tiles); b->d_tiles = nullptr; }
+}
+
+void* popp(sym_handle* h, int k) { return h->fast.pop[k]; }
+void* phip(sym_handle* h, int k) {
+  return h->fast.storage == SYM_STORE_FP64 ? (void*)h->fast.phi[k] : (void*)h->fast.phif[k];
+}
+
+DomainDesc make_desc(sym_handle* h, int cur, int pc) {
+  DomainDesc d;
+  std::memset(&d, 0, sizeof d);
+  d.P = h->dp;
+  d.pd = make_pad(h->dp);
+  d.pin = popp(h, cur);
+  d.pnext = popp(h, 1 - cur);
+  d.phic = phip(h, pc);
+  d.walls = h->walls;
+  d.walls_all = h->walls_all;
+  d.pout = h->pout;
+  d.Sp = h->dpart;
+  d.ffi = h->ffi;
+  d.solid = (h->dp.par > 0 || h->dp.wall_x) ? 1 : 0;
+  return d;
+}
+
+template <typename S>
+int capture_step(sym_batch* b, int k) {
+  const int n = (int)b->doms.size();
+  k_phase_batch<S><<<(unsigned)b->nblocks, 256, 0, b->st>>>(b->d_desc[k], b->d_blk_off, n);
+  for (int i = 0; i < n; i++) {
+    sym_handle* h = b->doms[i];
+    if (!(h->dp.par > 0 || h->dp.wall_x)) continue;
+    const int cur = (b->built_cur[i] + k) & 1, pc = (b->built_pc[i] + k) & 1;
+    cudaStream_t saved = h->st;
+    h->st = b->st;   // the domain's sparse kernels join the batch graph
+    const int e = fast_enqueue_sparse(h, cur, pc);
+    h->st = saved;
+    if (e) return berr(b, e, h->err.c_str());
+  }
+  cudaMemsetAsync(b->d_counter + k, 0, sizeof(int), b->st);
+  using R = typename Codec<S>::R;
+  k_collide_batch<S><<<b->grid, kTPB, sizeof(Smem<R>), b->st>>>(b->d_desc[k], b->d_tiles, b->ntiles,
+                                                                 b->d_counter + k);
+  return bcuda(b, cudaGetLastError(), "batch step");
+}
+
+// (re)build the descriptor and tile tables and both step graphs
+int build(sym_batch* b) {
+  free_graphs(b);
+  free_tables(b);
+  const int n = (int)b->doms.size();
+  b->built_cur.assign(n, 0);
+  b->built_pc.assign(n, 0);
+  std::vector<DomainDesc> desc[2];
+  std::vector<long long> off(n + 1, 0);
+  std::vector<TileEntry> tiles;
+  for (int i = 0; i < n; i++) {
+    sym_handle* h = b->doms[i];
+    if (!h->fast.valid) {
+      if (int e = fast_import(h)) return berr(b, e, h->err.c_str());
+      h->fast.valid = true;
+    }
+    b->built_cur[i] = h->fast.cur;
+    b->built_pc[i] = h->fast.pc;
+    for (int k = 0; k < 2; k++) desc[k].push_back(make_desc(h, (h->fast.cur + k) & 1, (h->fast.pc + k) & 1));
+    off[i + 1] = off[i] + (long long)((h->N + 255) / 256);
+    const int xc = std::max(1, b->xchunk[i]);
+    const DevParams& P = h->dp;
+    for (int xa = 0; xa < P.nx; xa += xc)
+      for (int y0 = 0; y0 < P.ny; y0 += BY)
+        for (int z0 = 0; z0 < P.nz; z0 += BZ) {
+          TileEntry e{};
+          e.dom = i; e.z0 = z0; e.y0 = y0; e.xa = xa; e.xb = std::min(xa + xc, P.nx);
+          e.cost = std::min(BZ, P.nz - z0) * std::min(BY, P.ny - y0) * (e.xb - e.xa);
+          tiles.push_back(e);
+        }
+  }
+  // largest tiles first: the persistent CTAs then finish together
+  std::stable_sort(tiles.begin(), tiles.end(), [](const TileEntry& a, const TileEntry& c) { return a.cost > c.cost; });
+  b->ntiles = (int)tiles.size();
+  b->nblocks = off[n];
+  for (int k = 0; k < 2; k++) {
+    if (int e = bcuda(b, cudaMalloc(&b->d_desc[k], sizeof(DomainDesc) * n), "descriptors")) return e;
+    cudaMemcpyAsync(b->d_desc[k], desc[k].data(), sizeof(DomainDesc) * n, cudaMemcpyHostToDevice, b->st);
+  }
+  if (int e = bcuda(b, cudaMalloc(&b->d_blk_off, sizeof(long long) * (n + 1)), "offsets")) return e;
+  cudaMemcpyAsync(b->d_blk_off, off.data(), sizeof(long long) * (n + 1), cudaMemcpyHostToDevice, b->st);
+  if (int e = bcuda(b, cudaMalloc(&b->d_tiles, sizeof(TileEntry) * std::max(1, b->ntiles)), "tiles")) return e;
+  cudaMemcpyAsync(b->d_tiles, tiles.data(), sizeof(TileEntry) * b->ntiles, cudaMemcpyHostToDevice, b->st);
+  if (int e = bcuda(b, cudaStreamSynchronize(b->st), "tables")) return e;
+  for (int k = 0; k < 2; k++) {
+    if (int e = bcuda(b, cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal), "capture")) return e;
+    int e1 = b->storage == SYM_STORE_FP64 ? capture_step<double>(b, k)
+           : b->storage == SYM_STORE_FP32 ? capture_step<float>(b, k) : capture_step<__half>(b, k);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(b->st, &g);
+    if (e1) { if (g) cudaGraphDestroy(g); return e1; }
+    if (int e = bcuda(b, e2, "end capture")) return e;
+    b->graph[k] = g;
+    if (int e = bcuda(b, cudaGraphInstantiate(&b->gexec[k], g, 0), "instantiate")) return e;
+  }
+  b->steps_since_build = 0;
+  b->built = true;
+  return SYM_OK;
+}
+
+// members stepped or exported outside the batch invalidate the graphs
+bool stale(sym_batch* b) {
+  if (!b->built) return true;
+  for (size_t i = 0; i < b->doms.size(); i++) {
+    const sym_handle* h = b->doms[i];
+    if (!h->fast.valid) return true;
+    if (h->fast.cur != ((b->built_cur[i] + b->steps_since_build) & 1)) return true;
+    if (h->fast.pc != ((b->built_pc[i] + b->steps_since_build) & 1)) return true;
+  }
+  return false;
+}
+
+int launch_steps(sym_batch* b, int nsteps) {
+  for (int t = 0; t < nsteps; t++) {
+    const int k = b->steps_since_build & 1;
+    if (int e = bcuda(b, cudaGraphLaunch(b->gexec[k], b->st), "graph launch")) return e;
+    b->steps_since_build++;
+    for (sym_handle* h : b->doms) {
+      h->fast.cur ^= 1;
+      h->fast.pc ^= 1;
+    }
+  }
+  return SYM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sym_batch_create(sym_handle* const* handles, int n, sym_batch** out) {
+  if (!out || !handles || n <= 0) return SYM_ERR_PARAM;
+  *out = nullptr;
+  sym_batch* b = new sym_batch();
+  b->device = handles[0]->device;
+  b->storage = handles[0]->fast.storage;
+  for (int i = 0; i < n; i++) {
+    sym_handle* h = handles[i];
+    if (!h || h->dp.ref || h->fast.storage < 0 || h->device != b->device || h->fast.storage != b->storage) {
+      delete b;
+      return SYM_ERR_PARAM;
+    }
+    b->doms.push_back(h);
+    b->xchunk.push_back(32);
+  }
+  cudaSetDevice(b->device);
+  int e = bcuda(b, cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking), "stream");
+  if (!e) e = bcuda(b, cudaMalloc(&b->d_counter, 2 * sizeof(int)), "counter");
+  if (!e) {
+    e = b->storage == SYM_STORE_FP64 ? set_batch_smem<double>(b->st, &b->grid, b->device)
+      : b->storage == SYM_STORE_FP32 ? set_batch_smem<float>(b->st, &b->grid, b->device)
+                                     : set_batch_smem<__half>(b->st, &b->grid, b->device);
+  }
+  if (e) {
+    fprintf(stderr, "sym_batch_create: %s\n", b->err.c_str());
+    if (b->d_counter) cudaFree(b->d_counter);
+    if (b->st) cudaStreamDestroy(b->st);
+    delete b;
+    return e;
+  }
+  *out = b;
+  return SYM_OK;
+}
+
+int sym_batch_destroy(sym_batch* b) {
+  if (!b) return SYM_OK;
+  cudaSetDevice(b->device);
+  if (b->st) cudaStreamSynchronize(b->st);
+  free_graphs(b);
+  free_tables(b);
+  if (b->d_counter) cudaFree(b->d_counter);
+  if (b->st) cudaStreamDestroy(b->st);
+  delete b;
+  return SYM_OK;
+}
+
+const char* sym_batch_last_error(const sym_batch* b) { return b ? b->err.c_str() : "null batch"; }
+
+int sym_batch_set_xchunk(sym_batch* b, int domain, int xchunk) {
+  if (!b || domain < 0 || domain >= (int)b->doms.size() || xchunk < 1) return SYM_ERR_PARAM;
+  if (b->xchunk[domain] != xchunk) {
+    b->xchunk[domain] = xchunk;
+    free_graphs(b);
+  }
+  return SYM_OK;
+}
+
+int sym_batch_get_xchunk(sym_batch* b, int domain, int* xchunk) {
+  if (!b || !xchunk || domain < 0 || domain >= (int)b->doms.size()) return SYM_ERR_PARAM;
+  *xchunk = b->xchunk[domain];
+  return SYM_OK;
+}
+
+int sym_batch_step(sym_batch* b, int nsteps) {
+  if (!b || nsteps < 0) return SYM_ERR_PARAM;
+  cudaSetDevice(b->device);
+  if (stale(b))
+    if (int e = build(b)) return e;
+  if (int e = launch_steps(b, nsteps)) return e;
+  return bcuda(b, cudaStreamSynchronize(b->st), "batch step");
+}
+
+int sym_batch_step_timed(sym_batch* b, int nsteps, double* ms) {
+  if (!b || !ms || nsteps <= 0) return SYM_ERR_PARAM;
+  cudaSetDevice(b->device);
+  if (stale(b))
+    if (int e = build(b)) return e;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, b->st);
+  int rc = launch_steps(b, nsteps);
+  cudaEventRecord(e1, b->st);
+  if (!rc) rc = bcuda(b, cudaStreamSynchronize(b->st), "batch timed");
+  float v = 0.f;
+  if (!rc) cudaEventElapsedTime(&v, e0, e1);
+  *ms = v;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
+}
+
+// Choose the tile x extent per size class (domains grouped by nx: <=32, <=48,
+// larger) from {8, 16, 32, 64} by timing trial_steps graph steps per
+// candidate.  The trial steps advance every domain; *steps_taken reports how
+// many.
+int sym_batch_autotune(sym_batch* b, int trial_steps, int* steps_taken) {
+  if (!b || trial_steps <= 0) return SYM_ERR_PARAM;
+  const int cands[4] = {8, 16, 32, 64};
+  auto cls = [](int nx) { return nx <= 32 ? 0 : (nx <= 48 ? 1 : 2); };
+  int taken = 0;
+  for (int c = 0; c < 3; c++) {
+    bool any = false;
+    for (sym_handle* h : b->doms) any |= cls(h->dp.nx) == c;
+    if (!any) continue;
+    double best = 1e300;
+    int bestx = 32;
+    for (int x : cands) {
+      for (size_t i = 0; i < b->doms.size(); i++)
+        if (cls(b->doms[i]->dp.nx) == c) sym_batch_set_xchunk(b, (int)i, x);
+      double ms = 0;
+      if (int e = sym_batch_step(b, 1)) return e;   // build + warm
+      taken += 1;
+      if (int e = sym_batch_step_timed(b, trial_steps, &ms)) return e;
+      taken += trial_steps;
+      if (ms < best) { best = ms; bestx = x; }
+    }
+    for (size_t i = 0; i < b->doms.size(); i++)
+      if (cls(b->doms[i]->dp.nx) == c) sym_batch_set_xchunk(b, (int)i, bestx);
+  }
+  if (steps_taken) *steps_taken = taken;
+  return SYM_OK;
+}
+
+int sym_batch_info(sym_batch* b, int64_t* nodes, int* ntiles, int* grid) {
+  if (!b) return SYM_ERR_PARAM;
+  long long n = 0;
+  for (sym_handle* h : b->doms) n += (long long)h->N;
+  if (nodes) *nodes = n;
+  if (ntiles) *ntiles = b->ntiles;
+  if (grid) *grid = b->grid;
+  return SYM_OK;
+}
+
+}  // extern "C"

@@ -113,6 +113,15 @@ int32_t* field_ptr_i(sym_handle* h, int f) {
   }
 }
 
+// Allocate the canonical arrays a CONFIG handle defers (fi, ffi, ft).
+int ensure_full(sym_handle* h) {
+  double** pops[3] = {&h->fi, &h->ffi, &h->ft};
+  for (auto pp : pops)
+    if (!*pp)
+      if (int e = dalloc(h, pp, 19 * h->N)) return e;
+  return SYM_OK;
+}
+
 // Make the canonical arrays authoritative (export the fused state if it holds
 // the current populations).
 int canonical(sym_handle* h) {
@@ -228,13 +237,15 @@ int sym_params_check(const sym_params* p, char* msg, size_t msg_len) {
 int sym_footprint(const sym_params* p, size_t* bytes) {
   if (!p || !bytes) return SYM_ERR_PARAM;
   const size_t N = (size_t)p->nx * p->ny * p->nz;
-  size_t b = 5 * 19 * N * 8 + 13 * N * 8 + 6 * N * 4 + reduction_len(*p) * 8 + sizeof(sym_particles);
+  const bool full = p->mode == SYM_MODE_REFERENCE || p->par > 0;
+  size_t b = (full ? 5 : 2) * 19 * N * 8 + 13 * N * 8 + 6 * N * 4 + reduction_len(*p) * 8 + sizeof(sym_particles);
   const int lam = p->la_m > 0 ? p->la_m : (p->alpha > 0 ? (int)(2.0 * M_PI / p->alpha) : 0);
   const int lan = p->la_n > 0 ? p->la_n : (p->alpha > 0 ? (int)(M_PI / p->alpha) : 0);
   b += (size_t)p->par * lam * (lan + 1) * (8 * 8 + 4);
   if (p->mode == SYM_MODE_CONFIG) {
     const size_t s = p->storage == SYM_STORE_FP64 ? 8 : (p->storage == SYM_STORE_FP32 ? 4 : 2);
-    b += 2 * 38 * N * s + 2 * N * 8;
+    const size_t pad = (size_t)(p->nx + 4) * (p->ny + 4) * ((p->nz + 4 + 3) / 4 * 4);
+    b += 2 * 38 * N * s + 2 * pad * (p->storage == SYM_STORE_FP64 ? 8 : 4);
   }
   *bytes = b;
   return SYM_OK;
@@ -256,9 +267,13 @@ int sym_create(const sym_params* p, int device, sym_handle** out) {
   int e = check_cuda(h, cudaSetDevice(device), "cudaSetDevice");
   if (!e) e = check_cuda(h, cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking), "stream");
   const size_t N = h->N;
-  double** pops[5] = {&h->ri, &h->bi, &h->fi, &h->ffi, &h->ft};
+  // ri, bi always; fi, ffi and the streaming/transfer temporary ft only where
+  // the mode needs them up front (REFERENCE subroutines, particle coupling),
+  // otherwise on the first call that uses them (ensure_full)
+  double** pops[2] = {&h->ri, &h->bi};
   for (auto pp : pops)
     if (!e) e = dalloc(h, pp, 19 * N);
+  if (!e && (p->mode == SYM_MODE_REFERENCE || p->par > 0)) e = ensure_full(h);
   double** sc[13] = {&h->rho, &h->ux, &h->uy, &h->uz, &h->rhoN, &h->rhoR, &h->rhoB,
                      &h->nx, &h->ny, &h->nz, &h->gx, &h->gy, &h->gz};
   for (auto pp : sc)
@@ -326,6 +341,7 @@ int sym_set_field(sym_handle* h, int field, const void* host) {
   if (int e = canonical(h)) return e;
   const size_t N = h->N;
   if (field >= SYM_F_RI && field <= SYM_F_FFI) {
+    if (int e = ensure_full(h)) return e;
     cudaMemcpyAsync(h->ft, host, sizeof(double) * 19 * N, cudaMemcpyHostToDevice, h->st);
     if (int e = aos_to_soa(h, h->ft, field_ptr_d(h, field))) return e;
   } else if (double* d = field_ptr_d(h, field)) {
@@ -344,6 +360,7 @@ int sym_get_field(sym_handle* h, int field, void* host) {
   if (int e = canonical(h)) return e;
   const size_t N = h->N;
   if (field >= SYM_F_RI && field <= SYM_F_FFI) {
+    if (int e = ensure_full(h)) return e;
     if (int e = soa_to_aos(h, field_ptr_d(h, field), h->ft)) return e;
     cudaMemcpyAsync(host, h->ft, sizeof(double) * 19 * N, cudaMemcpyDeviceToHost, h->st);
   } else if (double* d = field_ptr_d(h, field)) {
@@ -359,6 +376,7 @@ int sym_get_field(sym_handle* h, int field, void* host) {
 int sym_set_populations(sym_handle* h, const double* ri, const double* bi) {
   if (int e = guard(h)) return e;
   if (!ri || !bi) return set_error(h, SYM_ERR_PARAM, "null populations");
+  if (int e = ensure_full(h)) return e;
   if (h->fast.valid) {
     // both colours are replaced: only the fused phase field is still needed
     if (int e = fast_export(h)) return e;
@@ -444,6 +462,7 @@ int sym_init_slab(sym_handle* h, double z0, double z1, double width, double nois
 #define SYM_SUBROUTINE(name, call)                                     \
   int name(sym_handle* h) {                                            \
     if (int e = guard(h)) return e;                                    \
+    if (int e = ensure_full(h)) return e;                              \
     if (int e = canonical(h)) return e;                                \
     if (int e = call) return e;                                        \
     return check_cuda(h, cudaStreamSynchronize(h->st), #name);         \
@@ -466,6 +485,7 @@ SYM_SUBROUTINE(sym_refilling, part_refilling(h))
 int sym_streaming(sym_handle* h, int which) {
   if (int e = guard(h)) return e;
   if (which != 0 && which != 1) return set_error(h, SYM_ERR_PARAM, "streaming: which must be 0 (ri) or 1 (bi)");
+  if (int e = ensure_full(h)) return e;
   if (int e = canonical(h)) return e;
   if (int e = ref_streaming(h, which)) return e;
   return check_cuda(h, cudaStreamSynchronize(h->st), "sym_streaming");
@@ -482,6 +502,7 @@ int sym_step(sym_handle* h, int nsteps) {
     }
     return fast_step(h, nsteps);
   }
+  if (int e = ensure_full(h)) return e;
   if (int e = canonical(h)) return e;
   return canonical_steps(h, nsteps);
 }

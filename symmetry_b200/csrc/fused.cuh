@@ -1,0 +1,571 @@
+// fused.cuh -- device code of the fused fast path, shared by the
+// single-domain driver (fast.cu) and the batch engine (batch.cu).
+// See fast.cu for the per-step kernel sequence.
+#pragma once
+#include <cuda_fp16.h>
+#include <cmath>
+#include <utility>
+#include "state.cuh"
+
+namespace symb200 {
+namespace fused {
+
+constexpr int BZ = 32, BY = 8, TPB = BZ * BY;
+constexpr int XCHUNK = 32;   // x planes marched by one CTA
+
+// ---- halo-padded phase field -----------------------------------------------------
+struct Pad {
+  int nxp, nyp, nzp;
+  __host__ __device__ long long idx(int x, int y, int z) const {
+    return (long long)(z + 2) + (long long)nzp * ((long long)(y + 2) + (long long)nyp * (long long)(x + 2));
+  }
+  __host__ __device__ long long size() const { return (long long)nxp * nyp * nzp; }
+};
+inline Pad make_pad(const DevParams& P) {
+  Pad d;
+  d.nxp = P.nx + 4;
+  d.nyp = P.ny + 4;
+  d.nzp = ((P.nz + 4) + 3) / 4 * 4;   // row stride a multiple of 16 bytes
+  return d;
+}
+
+// store v at (x,y,z) and at each periodic image inside the 2-deep ghost layers
+template <typename R>
+__device__ __forceinline__ void phi_store(const DevParams& P, const Pad& pd, R* phi, int x, int y, int z, R v) {
+  int xs[3], ys[3], zs[3], nx = 1, ny = 1, nz = 1;
+  xs[0] = x; ys[0] = y; zs[0] = z;
+  if (x < 2) xs[nx++] = x + P.nx;
+  if (x >= P.nx - 2) xs[nx++] = x - P.nx;
+  if (y < 2) ys[ny++] = y + P.ny;
+  if (y >= P.ny - 2) ys[ny++] = y - P.ny;
+  if (z < 2) zs[nz++] = z + P.nz;
+  if (z >= P.nz - 2) zs[nz++] = z - P.nz;
+  for (int a = 0; a < nx; a++)
+    for (int b = 0; b < ny; b++)
+      for (int c = 0; c < nz; c++) phi[pd.idx(xs[a], ys[b], zs[c])] = v;
+}
+
+// ---- population storage codecs --------------------------------------------------
+// Slot 0 and slot 1 of each velocity hold (r, b) for FP64/FP32; for the
+// 16-bit storage they hold q = f/(w rho0) - 1 (FP16 shifted storage) and the
+// colour fraction c = r/f (16-bit fixed point).
+// Indices are 32-bit element offsets (the fused path requires 38*N < 2^32).
+// load takes rho0, store takes 1/rho0 (only the FP16 codec uses them).
+template <typename S>
+struct Codec;
+template <>
+struct Codec<double> {
+  using R = double;
+  template <int I>
+  __device__ __forceinline__ static void load(const double* __restrict__ p, unsigned N, unsigned L, R, R& r, R& b) {
+    r = p[I * N + L];
+    b = p[(19 + I) * N + L];
+  }
+  template <int I>
+  __device__ __forceinline__ static void store(double* p, unsigned N, unsigned L, R, R r, R f) {
+    p[I * N + L] = r;
+    p[(19 + I) * N + L] = f - r;
+  }
+};
+template <>
+struct Codec<float> {
+  using R = float;
+  template <int I>
+  __device__ __forceinline__ static void load(const float* __restrict__ p, unsigned N, unsigned L, R, R& r, R& b) {
+    r = p[I * N + L];
+    b = p[(19 + I) * N + L];
+  }
+  template <int I>
+  __device__ __forceinline__ static void store(float* p, unsigned N, unsigned L, R, R r, R f) {
+    p[I * N + L] = r;
+    p[(19 + I) * N + L] = f - r;
+  }
+};
+// FP16 shifted storage: slot 0 holds q = f/(w rho0) - 1 as FP16 (the deviation
+// of the total population from its rest equilibrium w rho0); slot 1 holds the
+// colour fraction c = r/f as 16-bit fixed point k = 16384 + 32768 c over
+// c in [-0.5, 1.5) (step 3.05e-5; the pure phases c = 0 and c = 1 are the
+// exact codes 16384 and 49152).
+template <>
+struct Codec<__half> {
+  using R = float;
+  template <int I>
+  __device__ __forceinline__ static void load(const __half* __restrict__ p, unsigned N, unsigned L, R rho0, R& r,
+                                              R& b) {
+    const R q = __half2float(p[I * N + L]);
+    const unsigned short k = reinterpret_cast<const unsigned short*>(p)[(19 + I) * N + L];
+    const R c = fmaf((R)k, 1.0f / 32768.0f, -0.5f);
+    const R f = (R(W(I)) * rho0) * (R(1) + q);
+    r = f * c;
+    b = f - r;
+  }
+  template <int I>
+  __device__ __forceinline__ static void store(__half* p, unsigned N, unsigned L, R irho0, R r, R f) {
+    const R q = f * (R(1.0 / W(I)) * irho0) - R(1);
+    const R c = __fdividef(r, f);
+    const R kf = fminf(fmaxf(fmaf(c, 32768.0f, 16384.0f), 0.0f), 65535.0f);
+    p[I * N + L] = __float2half_rn(q);
+    reinterpret_cast<unsigned short*>(p)[(19 + I) * N + L] = (unsigned short)__float2uint_rn(kf);
+  }
+};
+
+template <typename F, int... Is>
+__device__ __forceinline__ void unroll19_impl(F&& f, std::integer_sequence<int, Is...>) {
+  (f(std::integral_constant<int, Is>{}), ...);
+}
+template <typename F>
+__device__ __forceinline__ void unroll19(F&& f) {
+  unroll19_impl(f, std::make_integer_sequence<int, 19>{});
+}
+
+// ---- k_phase: calmacros (Source1.f90:770-831) on the fused state ------------------
+template <typename S, bool SOLID>
+__device__ __forceinline__ void phase_node(const DevParams& P, const Pad& pd, const S* __restrict__ pops,
+                                           typename Codec<S>::R* __restrict__ phi,
+                                           const int32_t* __restrict__ walls_all, long long L) {
+  using R = typename Codec<S>::R;
+  if (L >= P.N) return;
+  const int z = (int)(L % P.nz), y = (int)((L / P.nz) % P.ny), x = (int)(L / ((long long)P.nz * P.ny));
+  R v = R(0);
+  if (!(SOLID && walls_all[L] >= 1)) {
+    const unsigned N = (unsigned)P.N;
+    const R rho0 = R(P.rho0);
+    R sr = R(0), sb = R(0);
+    unroll19([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      R r, b;
+      Codec<S>::template load<i>(pops, N, (unsigned)L, rho0, r, b);
+      sr = sr + r;
+      sb = sb + b;
+    });
+    v = (sr - sb) / (sr + sb);
+  }
+  phi_store<R>(P, pd, phi, x, y, z, v);
+}
+
+template <typename S, bool SOLID>
+__global__ void __launch_bounds__(256) k_phase(DevParams P, Pad pd, const S* __restrict__ pops,
+                                               typename Codec<S>::R* __restrict__ phi,
+                                               const int32_t* __restrict__ walls_all) {
+  phase_node<S, SOLID>(P, pd, pops, phi, walls_all, blockIdx.x * 256LL + threadIdx.x);
+}
+
+// ---- wetting rotation of a node normal (derivatives :535-587) ---------------------
+template <typename R>
+__device__ __forceinline__ void wet_rotate(const DevParams& P, const sym_particles* S, int pp, int x, int y, int z,
+                                           R& n0, R& n1, R& n2) {
+  double nwd[3];
+  wall_normal_dev(P, S, pp, x, y, z, nwd);
+  const R nw[3] = {R(nwd[0]), R(nwd[1]), R(nwd[2])};
+  const R n[3] = {n0, n1, n2};
+  R v[3];
+  akai_rotate<R>(R(P.cita), nw, n, true, v);
+  n0 = v[0]; n1 = v[1]; n2 = v[2];
+}
+
+// ---- k_collide ------------------------------------------------------------------
+// phi ring of 5 planes and normal ring of 4 planes: with normals computed one
+// plane ahead and phi loaded three planes ahead, one barrier per plane keeps
+// every slot a warp may still read distinct from the slots being written.
+template <typename R>
+struct Smem {
+  R phi[5][BY + 4][BZ + 4];
+  R n[4][4][BY + 2][BZ + 2];   // [plane][nx,ny,nz,|grad|][y][z]
+};
+
+// One tile: the 32(z) x 8(y) footprint at (z0, y0), planes xa..xb-1.  Called
+// by the single-domain kernel (tile from blockIdx) and by the batched
+// persistent kernel (tile from the work-tile table).
+template <typename S, bool SOLID>
+__device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, const S* __restrict__ pin_,
+                                             S* __restrict__ pout_, const typename Codec<S>::R* __restrict__ phi,
+                                             const int32_t* __restrict__ walls,
+                                             const int32_t* __restrict__ walls_all,
+                                             const int32_t* __restrict__ pout,
+                                             const sym_particles* __restrict__ Sp, double* __restrict__ ffi,
+                                             int z0, int y0, int xa, int xb, Smem<typename Codec<S>::R>& sm) {
+  using R = typename Codec<S>::R;
+  const int tz = threadIdx.x % BZ, ty = threadIdx.x / BZ;
+  const unsigned N = (unsigned)P.N;
+  const R rho0 = R(P.rho0), irho0 = R(1.0 / P.rho0);
+  const R evap = R(P.evap);
+  const int sy = P.nz, sx = P.nz * P.ny;   // element strides of y and x
+
+  // load phi plane xp (padded coordinates stay inside the ghost layers)
+  auto load_phi = [&](int xp) {
+    R(*dst)[BZ + 4] = sm.phi[((xp % 5) + 5) % 5];
+    for (int t = threadIdx.x; t < (BY + 4) * (BZ + 4); t += TPB) {
+      const int py = t / (BZ + 4), pz = t % (BZ + 4);
+      const int y = y0 - 2 + py, z = z0 - 2 + pz;
+      R v = R(0);
+      if (y <= P.ny + 1 && z <= P.nz + 1) v = phi[pd.idx(xp, y, z)];
+      dst[py][pz] = v;
+    }
+  };
+  // unit normal (rotated at wetting nodes) and |grad phi| of plane xp, halo 1
+  auto compute_n = [&](int xp) {
+    const int s = ((xp % 4) + 4) % 4;
+    for (int t = threadIdx.x; t < (BY + 2) * (BZ + 2); t += TPB) {
+      const int py = t / (BZ + 2), pz = t % (BZ + 2);
+      const int y = y0 - 1 + py, z = z0 - 1 + pz;
+      R n0 = R(0), n1 = R(0), n2 = R(0), fn = R(0);
+      bool ok = y <= P.ny && z <= P.nz;
+      int pp = 0;
+      if (SOLID && ok) {
+        const unsigned Lw = (unsigned)(wrapi(z, P.nz) + sy * wrapi(y, P.ny) + sx * wrapi(xp, P.nx));
+        if (walls_all[Lw] > 0) ok = false;
+        else pp = pout[Lw];
+      }
+      if (ok) {
+        R g0 = R(0), g1 = R(0), g2 = R(0);
+#pragma unroll
+        for (int i = 1; i < 19; i++) {
+          const R val = R(W(i)) * sm.phi[(((xp + CX(i)) % 5) + 5) % 5][py + 1 + CY(i)][pz + 1 + CZ(i)];
+          if (CX(i)) g0 = g0 + val * R(CX(i));
+          if (CY(i)) g1 = g1 + val * R(CY(i));
+          if (CZ(i)) g2 = g2 + val * R(CZ(i));
+        }
+        g0 = R(3) * g0; g1 = R(3) * g1; g2 = R(3) * g2;
+        fn = sqrt(g0 * g0 + g1 * g1 + g2 * g2);
+        if (fn > evap) {
+          const R rf = R(1) / fn;
+          n0 = g0 * rf; n1 = g1 * rf; n2 = g2 * rf;
+          if (SOLID && pp >= 1) wet_rotate<R>(P, Sp, pp, wrapi(xp, P.nx), wrapi(y, P.ny), wrapi(z, P.nz), n0, n1, n2);
+        } else {
+          fn = R(0);
+        }
+      }
+      sm.n[s][0][py][pz] = n0; sm.n[s][1][py][pz] = n1; sm.n[s][2][py][pz] = n2; sm.n[s][3][py][pz] = fn;
+    }
+  };
+
+  load_phi(xa - 2); load_phi(xa - 1); load_phi(xa); load_phi(xa + 1); load_phi(xa + 2);
+  __syncthreads();
+  compute_n(xa - 1);
+  compute_n(xa);
+  // the first iteration's phi load reuses the slot of plane xa-2, which
+  // compute_n(xa-1) above reads
+  __syncthreads();
+
+  const int y = y0 + ty, z = z0 + tz;
+  for (int x = xa; x < xb; x++) {
+    // normals of plane x+1 (phi planes x..x+2 are resident) and phi of plane x+3
+    compute_n(x + 1);
+    if (x + 3 <= xb + 1) load_phi(x + 3);
+    __syncthreads();
+    if (y >= P.ny || z >= P.nz) continue;
+    const unsigned L = (unsigned)(z + sy * y + sx * x);
+    if (x + 1 < xb) {
+      // bring the next plane's populations toward L2 while this plane computes
+#pragma unroll
+      for (int i = 0; i < 38; i++) asm volatile("prefetch.global.L2 [%0];" ::"l"(pin_ + (i * N + L + sx)));
+    }
+    int pp = 0;
+    if (SOLID) {
+      if (walls_all[L] > 0) continue;
+      pp = pout[L];
+    }
+    // calmacros on the own populations
+    R f[19];
+    R sr = R(0), sb = R(0);
+    unroll19([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      R r, b;
+      Codec<S>::template load<i>(pin_, N, L, rho0, r, b);
+      f[i] = r + b;
+      sr = sr + r;
+      sb = sb + b;
+    });
+    const R rho = sr + sb;
+    R ux = R(0), uy = R(0), uz = R(0);
+#pragma unroll
+    for (int i = 0; i < 19; i++) {
+      if (CX(i)) ux = ux + f[i] * R(CX(i));
+      if (CY(i)) uy = uy + f[i] * R(CY(i));
+      if (CZ(i)) uz = uz + f[i] * R(CZ(i));
+    }
+    ux = ux / rho; uy = uy / rho; uz = uz / rho;
+    const int s1 = x % 4;
+    const R nx = sm.n[s1][0][ty + 1][tz + 1], ny = sm.n[s1][1][ty + 1][tz + 1], nz = sm.n[s1][2][ty + 1][tz + 1];
+    const R fn = sm.n[s1][3][ty + 1][tz + 1];
+    const bool flag = fn > evap;
+    const R rhoN = sm.phi[x % 5][ty + 2][tz + 2];
+    // CSF surface tension from the curvature of the normal field (:624-667)
+    R fx = R(0), fy = R(0), fz = R(0);
+    if (flag && (!SOLID || pp <= 0)) {
+      R d00 = 0, d01 = 0, d02 = 0, d10 = 0, d11 = 0, d12 = 0, d20 = 0, d21 = 0, d22 = 0;
+#pragma unroll
+      for (int i = 1; i < 19; i++) {
+        const int sl = (x + CX(i) + 4) % 4;
+        const int yy = ty + 1 + CY(i), zz = tz + 1 + CZ(i);
+        const R a = R(W(i)) * sm.n[sl][0][yy][zz];
+        const R b = R(W(i)) * sm.n[sl][1][yy][zz];
+        const R c = R(W(i)) * sm.n[sl][2][yy][zz];
+        if (CX(i)) { d00 = d00 + a * R(CX(i)); d10 = d10 + b * R(CX(i)); d20 = d20 + c * R(CX(i)); }
+        if (CY(i)) { d01 = d01 + a * R(CY(i)); d11 = d11 + b * R(CY(i)); d21 = d21 + c * R(CY(i)); }
+        if (CZ(i)) { d02 = d02 + a * R(CZ(i)); d12 = d12 + b * R(CZ(i)); d22 = d22 + c * R(CZ(i)); }
+      }
+      d00 *= R(3); d01 *= R(3); d02 *= R(3); d10 *= R(3); d11 *= R(3); d12 *= R(3);
+      d20 *= R(3); d21 *= R(3); d22 *= R(3);
+      const R kurv = nx * ny * (d10 + d01) + nx * nz * (d20 + d02) + ny * nz * (d12 + d21) -
+                     (ny * ny + nz * nz) * d00 - (nx * nx + nz * nz) * d11 - (nx * nx + ny * ny) * d22;
+      const R val = R(0.5) * R(P.sigma) * kurv;
+      fx = val * (fn * nx); fy = val * (fn * ny); fz = val * (fn * nz);
+    }
+    fx = fx + rho * R(P.body[0]);
+    fy = fy + rho * R(P.body[1]);
+    fz = fz + rho * R(P.body[2]);
+    ux = ux + R(0.5) * fx / rho;
+    uy = uy + R(0.5) * fy / rho;
+    uz = uz + R(0.5) * fz / rho;
+    mrt_collide<R>(P, f, rho, ux, uy, uz, fx, fy, fz, rhoN);
+    if (SOLID && pp >= 1) {
+#pragma unroll
+      for (int i = 0; i < 19; i++) ffi[(size_t)i * N + L] = (double)f[i];
+    }
+    // Latva-Kokko recolouring (:712-726) and push streaming with bounce-back
+    const R ratio = sr / rho;
+    const R coef = sr * sb / rho * R(P.beta);
+    const bool rzero = sr <= evap, bzero = sb <= evap;
+    // neighbour offsets with the periodic wrap folded in (one select per face)
+    const int oxp = (x == P.nx - 1) ? -(P.nx - 1) * sx : sx, oxm = (x == 0) ? (P.nx - 1) * sx : -sx;
+    const int oyp = (y == P.ny - 1) ? -(P.ny - 1) * sy : sy, oym = (y == 0) ? (P.ny - 1) * sy : -sy;
+    const int ozp = (z == P.nz - 1) ? -(P.nz - 1) : 1, ozm = (z == 0) ? (P.nz - 1) : -1;
+    unroll19([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      R r = ratio * f[i];
+      if (i > 0 && flag) r = r + coef * R(W(i)) * (nx * R(CX(i)) + ny * R(CY(i)) + nz * R(CZ(i)));
+      if (rzero) r = R(0);
+      if (bzero) r = f[i];
+      const unsigned T = L + (CX(i) > 0 ? oxp : (CX(i) < 0 ? oxm : 0)) + (CY(i) > 0 ? oyp : (CY(i) < 0 ? oym : 0)) +
+                         (CZ(i) > 0 ? ozp : (CZ(i) < 0 ? ozm : 0));
+      if (SOLID && i > 0 && pp >= 1) {
+        const int wb = walls[T];
+        const bool flat = wb > P.par;
+        if (wb == pp || flat) {
+          // curve (:1001-1019): link OPC(i) of this node comes back reversed
+          constexpr int j = OPC(i);
+          R star = R(0);
+          if (!flat) {
+            const int par = P.par;
+            const R xr = R(disp(P, (double)(x + P.origin), Sp->center[0 * par + wb - 1], 0));
+            const R yr = R(disp(P, (double)(y + P.origin), Sp->center[1 * par + wb - 1], 1));
+            const R zr = R(disp(P, (double)(z + P.origin), Sp->center[2 * par + wb - 1], 2));
+            const R uw0 = R(Sp->up[0 * par + wb - 1]) + zr * R(Sp->rp[1 * par + wb - 1]) - yr * R(Sp->rp[2 * par + wb - 1]);
+            const R uw1 = R(Sp->up[1 * par + wb - 1]) + xr * R(Sp->rp[2 * par + wb - 1]) - zr * R(Sp->rp[0 * par + wb - 1]);
+            const R uw2 = R(Sp->up[2 * par + wb - 1]) + yr * R(Sp->rp[0 * par + wb - 1]) - xr * R(Sp->rp[1 * par + wb - 1]);
+            star = uw0 * R(CX(j)) + uw1 * R(CY(j)) + uw2 * R(CZ(j));
+          }
+          const R rr = r + R(6.0 * W(j)) * sr * star;
+          const R bb = (f[i] - r) + R(6.0 * W(j)) * sb * star;
+          Codec<S>::template store<j>(pout_, N, L, irho0, rr, rr + bb);
+          return;
+        }
+      }
+      Codec<S>::template store<i>(pout_, N, T, irho0, r, f[i]);
+    });
+  }
+}
+
+template <typename S, bool SOLID>
+__global__ void __launch_bounds__(TPB, 2) k_collide(DevParams P, Pad pd, const S* __restrict__ pin_,
+                                                   S* __restrict__ pout_,
+                                                   const typename Codec<S>::R* __restrict__ phi,
+                                                   const int32_t* __restrict__ walls,
+                                                   const int32_t* __restrict__ walls_all,
+                                                   const int32_t* __restrict__ pout,
+                                                   const sym_particles* __restrict__ Sp, double* __restrict__ ffi,
+                                                   int xchunk) {
+  using R = typename Codec<S>::R;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem<R>& sm = *reinterpret_cast<Smem<R>*>(smem_raw);
+  const int xa = blockIdx.z * xchunk;
+  collide_tile<S, SOLID>(P, pd, pin_, pout_, phi, walls, walls_all, pout, Sp, ffi, blockIdx.x * BZ, blockIdx.y * BY,
+                         xa, min(xa + xchunk, P.nx), sm);
+}
+
+// ---- pin fill on the fused state (derivatives :467-492) ----------------------------
+template <typename R>
+__global__ void k_fast_pinfill_plane(DevParams P, Pad pd, R* phi, const int32_t* __restrict__ pin,
+                                     const int32_t* __restrict__ walls_all, int xplane) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= P.ny * P.nz) return;
+  const int y = t / P.nz, z = t % P.nz, x = xplane;
+  const long long L = lin(P, x, y, z);
+  if (pin[L] <= 0) return;
+  R ws = R(0), v = R(0);
+#pragma unroll
+  for (int i = 1; i < 19; i++) {
+    const long long nb = lin(P, wrapi(x + CX(i), P.nx), wrapi(y + CY(i), P.ny), wrapi(z + CZ(i), P.nz));
+    if (walls_all[nb] <= 0) { ws = ws + R(W(i)); v = v + R(W(i)) * phi[pd.idx(x + CX(i), y + CY(i), z + CZ(i))]; }
+  }
+  phi_store<R>(P, pd, phi, x, y, z, v / ws);
+}
+
+// node of a particle box (origin from the device-resident centre; see particles.cu)
+__device__ __forceinline__ bool fbox_node(const DevParams& P, int n, double margin, const double* centre, int pp,
+                                          long long t, int& x, int& y, int& z) {
+  if (t >= (long long)n * n * n) return false;
+  int id[3];
+  id[2] = (int)(t % n);
+  t /= n;
+  id[1] = (int)(t % n);
+  id[0] = (int)(t / n);
+  const int dims[3] = {P.nx, P.ny, P.nz};
+  int v[3];
+  for (int k = 0; k < 3; k++) {
+    const double c = centre[k * P.par + pp - 1] - (double)P.origin;
+    int q = (int)floor(c - P.rad - margin) + id[k];
+    const bool periodic = !(k == 0 && P.wall_x);
+    if (n >= dims[k]) q = id[k];
+    if (q >= dims[k] && n >= dims[k]) return false;
+    if (periodic) q = ((q % dims[k]) + dims[k]) % dims[k];
+    else if (q < 0 || q >= dims[k]) return false;
+    v[k] = q;
+  }
+  x = v[0]; y = v[1]; z = v[2];
+  return true;
+}
+
+template <typename R>
+__global__ void k_fast_pinfill_box(DevParams P, Pad pd, int n, double margin, int pp,
+                                   const sym_particles* __restrict__ Sp, R* phi, const int32_t* __restrict__ pin,
+                                   const int32_t* __restrict__ walls_all) {
+  int x, y, z;
+  if (!fbox_node(P, n, margin, Sp->center, pp, blockIdx.x * (long long)blockDim.x + threadIdx.x, x, y, z)) return;
+  const long long L = lin(P, x, y, z);
+  if (pin[L] <= 0) return;
+  R ws = R(0), v = R(0);
+#pragma unroll
+  for (int i = 1; i < 19; i++) {
+    const long long nb = lin(P, wrapi(x + CX(i), P.nx), wrapi(y + CY(i), P.ny), wrapi(z + CZ(i), P.nz));
+    if (walls_all[nb] <= 0) { ws = ws + R(W(i)); v = v + R(W(i)) * phi[pd.idx(x + CX(i), y + CY(i), z + CZ(i))]; }
+  }
+  phi_store<R>(P, pd, phi, x, y, z, v / ws);
+}
+
+// ---- particle preparation: canonical views of the fused state on a particle box ----
+// rho_N (this step's calmacros), rho_R/rho_B and fi (current populations), and the
+// previous step's gradient/normal (from the previous pin-filled phi) -- what
+// Lagrange_points, momentum and refilling read.
+template <typename S>
+__global__ void k_fast_prep(DevParams P, Pad pd, int n, double margin, int pp, const sym_particles* __restrict__ Sp,
+                            const S* __restrict__ pops, const typename Codec<S>::R* __restrict__ phi_cur,
+                            const typename Codec<S>::R* __restrict__ phi_prev,
+                            const int32_t* __restrict__ walls_all, const int32_t* __restrict__ pout,
+                            double* rhoN, double* rhoR, double* rhoB, double* fi, double* gx, double* gy,
+                            double* gz, double* nxv, double* nyv, double* nzv) {
+  using R = typename Codec<S>::R;
+  int x, y, z;
+  if (!fbox_node(P, n, margin, Sp->center, pp, blockIdx.x * (long long)blockDim.x + threadIdx.x, x, y, z)) return;
+  const long long L = lin(P, x, y, z);
+  const unsigned N = (unsigned)P.N;
+  const R rho0 = R(P.rho0);
+  if (walls_all[L] > 0) {
+    rhoN[L] = 0.0;
+    gx[L] = 0.0; gy[L] = 0.0; gz[L] = 0.0; nxv[L] = 0.0; nyv[L] = 0.0; nzv[L] = 0.0;
+    return;
+  }
+  R sr = R(0), sb = R(0);
+  unroll19([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    R r, b;
+    Codec<S>::template load<i>(pops, N, (unsigned)L, rho0, r, b);
+    fi[(size_t)i * N + L] = (double)(r + b);
+    sr = sr + r;
+    sb = sb + b;
+  });
+  rhoR[L] = (double)sr; rhoB[L] = (double)sb;
+  rhoN[L] = (double)phi_cur[pd.idx(x, y, z)];
+  R g0 = R(0), g1 = R(0), g2 = R(0);
+#pragma unroll
+  for (int i = 1; i < 19; i++) {
+    const R val = R(W(i)) * phi_prev[pd.idx(x + CX(i), y + CY(i), z + CZ(i))];
+    if (CX(i)) g0 = g0 + val * R(CX(i));
+    if (CY(i)) g1 = g1 + val * R(CY(i));
+    if (CZ(i)) g2 = g2 + val * R(CZ(i));
+  }
+  g0 = R(3) * g0; g1 = R(3) * g1; g2 = R(3) * g2;
+  const R fn = sqrt(g0 * g0 + g1 * g1 + g2 * g2);
+  R n0 = R(0), n1 = R(0), n2 = R(0);
+  if (fn > R(P.evap)) {
+    n0 = g0 / fn; n1 = g1 / fn; n2 = g2 / fn;
+    const int q = pout[L];
+    if (q >= 1) {
+      wet_rotate<R>(P, Sp, q, x, y, z, n0, n1, n2);
+      g0 = fn * n0; g1 = fn * n1; g2 = fn * n2;
+    }
+  }
+  gx[L] = g0; gy[L] = g1; gz[L] = g2; nxv[L] = n0; nyv[L] = n1; nzv[L] = n2;
+}
+
+// after refilling: refilled nodes' canonical populations and phi into the fused state
+template <typename S>
+__global__ void k_fast_refill_import(DevParams P, Pad pd, int n, double margin, int pp,
+                                     const sym_particles* __restrict__ Sp, S* pops,
+                                     typename Codec<S>::R* phi_cur, const int32_t* __restrict__ pout,
+                                     const int32_t* __restrict__ walls_old, const double* __restrict__ ri,
+                                     const double* __restrict__ bi, const double* __restrict__ rhoN) {
+  using R = typename Codec<S>::R;
+  int x, y, z;
+  if (!fbox_node(P, n, margin, Sp->center_old, pp, blockIdx.x * (long long)blockDim.x + threadIdx.x, x, y, z))
+    return;
+  const long long L = lin(P, x, y, z);
+  const unsigned N = (unsigned)P.N;
+  if (pout[L] != pp || walls_old[L] < 1) return;
+  const R irho0 = R(1.0 / P.rho0);
+  unroll19([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    const R r = R(ri[(size_t)i * N + L]), b = R(bi[(size_t)i * N + L]);
+    Codec<S>::template store<i>(pops, N, (unsigned)L, irho0, r, r + b);
+  });
+  phi_store<R>(P, pd, phi_cur, x, y, z, R(rhoN[L]));
+}
+
+// whole-domain conversions between the canonical arrays and the fused state
+template <typename S>
+__global__ void k_import_pops(DevParams P, const double* __restrict__ ri, const double* __restrict__ bi, S* pops) {
+  using R = typename Codec<S>::R;
+  const long long L = blockIdx.x * 256LL + threadIdx.x;
+  if (L >= P.N) return;
+  const unsigned N = (unsigned)P.N;
+  const R irho0 = R(1.0 / P.rho0);
+  unroll19([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    const R r = R(ri[(size_t)i * N + L]), b = R(bi[(size_t)i * N + L]);
+    Codec<S>::template store<i>(pops, N, (unsigned)L, irho0, r, r + b);
+  });
+}
+template <typename S>
+__global__ void k_export_pops(DevParams P, const S* __restrict__ pops, double* ri, double* bi) {
+  using R = typename Codec<S>::R;
+  const long long L = blockIdx.x * 256LL + threadIdx.x;
+  if (L >= P.N) return;
+  const unsigned N = (unsigned)P.N;
+  const R rho0 = R(P.rho0);
+  unroll19([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    R r, b;
+    Codec<S>::template load<i>(pops, N, (unsigned)L, rho0, r, b);
+    ri[(size_t)i * N + L] = (double)r;
+    bi[(size_t)i * N + L] = (double)b;
+  });
+}
+template <typename R>
+__global__ void k_import_phi(DevParams P, Pad pd, const double* __restrict__ rhoN, R* phi) {
+  const long long L = blockIdx.x * 256LL + threadIdx.x;
+  if (L >= P.N) return;
+  const int z = (int)(L % P.nz), y = (int)((L / P.nz) % P.ny), x = (int)(L / ((long long)P.nz * P.ny));
+  phi_store<R>(P, pd, phi, x, y, z, R(rhoN[L]));
+}
+template <typename R>
+__global__ void k_export_phi(DevParams P, Pad pd, const R* __restrict__ phi, double* rhoN) {
+  const long long L = blockIdx.x * 256LL + threadIdx.x;
+  if (L >= P.N) return;
+  const int z = (int)(L % P.nz), y = (int)((L / P.nz) % P.ny), x = (int)(L / ((long long)P.nz * P.ny));
+  rhoN[L] = (double)phi[pd.idx(x, y, z)];
+}
+
+
+}  // namespace fused
+}  // namespace symb200

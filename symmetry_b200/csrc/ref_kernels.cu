@@ -382,7 +382,8 @@ __global__ void k_initialization(DevParams P, double* rhoN, double* rho, double*
 #pragma unroll
   for (int i = 0; i < 19; i++) {
     const double r = feq_srt<double>(i, R, 0.0, 0.0, 0.0, 0.0), b = feq_srt<double>(i, B, 0.0, 0.0, 0.0, 0.0);
-    ri[i * N + L] = r; bi[i * N + L] = b; fi[i * N + L] = r + b; ffi[i * N + L] = r + b;
+    ri[i * N + L] = r; bi[i * N + L] = b;
+    if (fi) { fi[i * N + L] = r + b; ffi[i * N + L] = r + b; }
   }
 }
 
@@ -399,7 +400,8 @@ __global__ void k_init_fill(DevParams P, const double* rhoN, const double* rho, 
 #pragma unroll
   for (int i = 0; i < 19; i++) {
     const double r = feq_srt<double>(i, R, 0.0, 0.0, 0.0, 0.0), b = feq_srt<double>(i, B, 0.0, 0.0, 0.0, 0.0);
-    ri[i * N + L] = r; bi[i * N + L] = b; fi[i * N + L] = r + b; ffi[i * N + L] = r + b;
+    ri[i * N + L] = r; bi[i * N + L] = b;
+    if (fi) { fi[i * N + L] = r + b; ffi[i * N + L] = r + b; }
   }
 }
 

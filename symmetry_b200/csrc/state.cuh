@@ -15,6 +15,7 @@ struct FastState {
   void* pop[2] = {nullptr, nullptr};
   int cur = 0;             // buffer holding the current post-stream populations
   int pc = 0;              // phase-field buffer written by the next step
+  int xchunk = 0;          // x planes per tile of the fused collide kernel (0 = default)
   double* phi[2] = {nullptr, nullptr};  // FP64 halo-padded phase field (pin-filled)
   float* phif[2] = {nullptr, nullptr};  // FP32 halo-padded phase field for FP32/FP16 storage
   bool valid = false;      // fast state holds the authoritative populations
@@ -96,4 +97,5 @@ int fast_import(sym_handle* h);   // canonical -> fast
 int fast_export(sym_handle* h);   // fast -> canonical
 int fast_step(sym_handle* h, int nsteps);
 int fast_step_timed(sym_handle* h, int nsteps, double ms[4]);
+int fast_enqueue_sparse(sym_handle* h, int cur, int pc);   // particles + pin fill on h->st
 }  // namespace symb200

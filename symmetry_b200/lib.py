@@ -73,6 +73,17 @@ def lib() -> ctypes.CDLL:
         L.sym_output3.argtypes = [H, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int32)]
         L.sym_neck_radius.argtypes = [H, ctypes.POINTER(ctypes.c_double)]
         L.sym_mass_momentum.argtypes = [H, ctypes.c_void_p]
+        L.sym_batch_create.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+        L.sym_batch_destroy.argtypes = [ctypes.c_void_p]
+        L.sym_batch_last_error.restype = ctypes.c_char_p
+        L.sym_batch_last_error.argtypes = [ctypes.c_void_p]
+        L.sym_batch_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.sym_batch_step_timed.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+        L.sym_batch_set_xchunk.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+        L.sym_batch_get_xchunk.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+        L.sym_batch_autotune.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+        L.sym_batch_info.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int),
+                                     ctypes.POINTER(ctypes.c_int)]
         L.sym_mass_momentum_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
                                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]
         _lib = L
@@ -220,6 +231,59 @@ class Lattice:
         out = np.zeros(5)
         self._ck(lib().sym_mass_momentum(self.h, out.ctypes.data), "mass_momentum")
         return out
+
+
+class Batch:
+    """Many Lattice domains stepped together (sym_batch_*)."""
+
+    def __init__(self, lattices):
+        self.members = list(lattices)
+        arr = (ctypes.c_void_p * len(self.members))(*[m.h.value for m in self.members])
+        self.b = ctypes.c_void_p()
+        rc = lib().sym_batch_create(arr, len(self.members), ctypes.byref(self.b))
+        if rc:
+            raise SymError(rc, "sym_batch_create: members must share device, CONFIG mode and storage")
+
+    def _ck(self, rc, what):
+        if rc:
+            raise SymError(rc, f"{what}: {lib().sym_batch_last_error(self.b).decode()}")
+
+    def step(self, n: int = 1):
+        self._ck(lib().sym_batch_step(self.b, n), "batch step")
+
+    def step_timed(self, n: int) -> float:
+        ms = ctypes.c_double()
+        self._ck(lib().sym_batch_step_timed(self.b, n, ctypes.byref(ms)), "batch step_timed")
+        return ms.value
+
+    def set_xchunk(self, i: int, x: int):
+        self._ck(lib().sym_batch_set_xchunk(self.b, i, x), "set_xchunk")
+
+    def xchunk(self, i: int) -> int:
+        v = ctypes.c_int()
+        self._ck(lib().sym_batch_get_xchunk(self.b, i, ctypes.byref(v)), "get_xchunk")
+        return v.value
+
+    def autotune(self, trial_steps: int = 5) -> int:
+        taken = ctypes.c_int()
+        self._ck(lib().sym_batch_autotune(self.b, trial_steps, ctypes.byref(taken)), "autotune")
+        return taken.value
+
+    def info(self):
+        n, t, g = ctypes.c_int64(), ctypes.c_int(), ctypes.c_int()
+        self._ck(lib().sym_batch_info(self.b, ctypes.byref(n), ctypes.byref(t), ctypes.byref(g)), "info")
+        return dict(nodes=n.value, tiles=t.value, grid=g.value)
+
+    def close(self):
+        if self.b:
+            lib().sym_batch_destroy(self.b)
+            self.b = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def setup_workload(w, device: int = 0) -> Lattice:
