@@ -220,12 +220,92 @@ int sym_batch_get_xchunk(sym_batch* b, int domain, int* xchunk);
  * {8,16,32,64} by timing; the trial steps advance every domain (*steps_taken). */
 int sym_batch_autotune(sym_batch* b, int trial_steps, int* steps_taken);
 int sym_batch_info(sym_batch* b, int64_t* nodes, int* ntiles, int* grid);
+/* nsteps eager batch steps (not the graph) with CUDA events on the batch
+ * stream: ms[0] = whole region, ms[1] = phase-field launches, ms[2] = the
+ * per-domain particle/wall chains (fork to join), ms[3] = collide launches. */
+int sym_batch_step_kernels(sym_batch* b, int nsteps, double ms[4]);
+/* Kernel launches in one captured batch step (kernel nodes of its graph). */
+int sym_batch_kernels_per_step(sym_batch* b, int* kernels);
+
+/* ---- serving: a continuous-batching job server -----------------------------
+ * No counterpart in the reference (it runs one job per process).  Jobs are
+ * CONFIG domains with their own geometry, viscosity, surface tension, contact
+ * angle, particle and stop rule.  The server admits pending jobs first come
+ * first served while their device footprint (sym_footprint) fits the byte
+ * budget and a slot is free, keeps admitted jobs resident on the device, and
+ * steps all running jobs of one storage mode as one batch (sym_batch_*),
+ * rebuilt when a job joins or leaves; batches of different storage modes run
+ * on their own streams and overlap.  Every `check_every` steps of a job the
+ * server reduces its phase field to r_eq(z) = sqrt(sum_xy (1+phi)/2 / pi) and
+ * retires the job when min_z r_eq falls below its stop radius (breakup, time
+ * interpolated linearly between the last two checks), when it reaches its
+ * step limit, or when the field is no longer finite (failed, SYM_ERR_NAN).
+ * Jobs are admitted only at multiples of `check_every` server steps, so a
+ * job's checks fall on the same steps whatever else runs beside it: its
+ * result is the one it gets alone.  One host thread drives a server through
+ * sym_server_tick. */
+#define SYM_JOB_THREAD 0   /* Rayleigh-Plateau thread along z (sym_init_thread) */
+#define SYM_JOB_SLAB   1   /* red slab z0 <= z <= z1 (sym_init_slab)            */
+
+#define SYM_JOB_PENDING 0
+#define SYM_JOB_RUNNING 1
+#define SYM_JOB_BREAKUP 2  /* done: min r_eq fell below stop_radius */
+#define SYM_JOB_LIMIT   3  /* done: reached max_steps                */
+#define SYM_JOB_FAILED  4  /* error (see sym_job_result.error)       */
+
+typedef struct sym_job_spec {
+  sym_params p;         /* CONFIG mode; p.storage selects the batch it joins     */
+  int32_t kind;         /* SYM_JOB_THREAD or SYM_JOB_SLAB                        */
+  int32_t max_steps;    /* step limit (> 0)                                      */
+  double gen[5];        /* THREAD: radius, amp, wavelength, width, noise;
+                           SLAB: z0, z1, width, noise, unused                     */
+  uint64_t seed;        /* phase-field noise seed                                */
+  double stop_radius;   /* breakup when min_z r_eq(z) < stop_radius (<= 0: 1.0)  */
+  double center[3];     /* particle centre (p.par == 1)                          */
+  double up[3];         /* particle velocity                                     */
+  double t_arrival;     /* arrival on the server clock in seconds; < 0 = now     */
+} sym_job_spec;
+
+typedef struct sym_job_result {
+  int32_t status;       /* SYM_JOB_*                                             */
+  int32_t error;        /* SYM_ERR_* when FAILED                                 */
+  int32_t steps;        /* lattice steps run                                     */
+  int32_t reserved;
+  double breakup_step;  /* interpolated breakup step; -1 if none                 */
+  double rmin;          /* min_z r_eq at the last check                          */
+  double t_arrival, t_admit, t_done;   /* server clock, seconds (-1 = not yet)   */
+  int64_t node_updates; /* nodes x steps                                         */
+} sym_job_result;
+
+typedef struct sym_server sym_server;
+/* budget_bytes: device bytes the resident jobs may hold (sum of footprints);
+ * slots: most jobs resident at once; check_every: stop-rule interval (<= 0: 10). */
+int sym_server_create(int device, size_t budget_bytes, int slots, int check_every, sym_server** out);
+int sym_server_destroy(sym_server* s);
+const char* sym_server_last_error(const sym_server* s);
+/* Queue a job; *id identifies it in sym_server_result. */
+int sym_server_submit(sym_server* s, const sym_job_spec* spec, int64_t* id);
+/* One round of the request loop: admit what fits, run every batch for up to
+ * max_steps steps (to the next check; <= 0: no cap), check, retire.  Returns
+ * after the device work of the round; *running and *pending may be NULL. */
+int sym_server_tick(sym_server* s, int max_steps, int* running, int* pending);
+int sym_server_result(sym_server* s, int64_t id, sym_job_result* out);
+/* Tile x extent used for jobs of one size class (0: nx <= 32, 1: <= 48,
+ * 2: larger) in the batches the server builds (default 32). */
+int sym_server_set_xchunk(sym_server* s, int size_class, int xchunk);
+/* out[0] node updates, [1] device milliseconds of the batch steps, [2] jobs
+ * done, [3] jobs failed, [4] running, [5] pending, [6] resident footprint
+ * bytes, [7] server clock in seconds. */
+int sym_server_stats(sym_server* s, double out[8]);
 
 /* ---- diagnostics ------------------------------------------------------- */
 /* output3 (Source1.f90:1673-1717): neck height hmin on plane x=xl-1 and the y
  * where it occurs (REFERENCE geometry). */
 int sym_output3(sym_handle* h, double* hmin, int32_t* y0);
-/* CONFIG stop rule: min over z of r_eq(z) = sqrt(sum_xy (1+phi)/2 / pi). */
+/* CONFIG stop rule: min over z of r_eq(z) = sqrt(sum_xy (1+phi)/2 / pi) over
+ * fluid nodes.  After sym_step in CONFIG mode it reduces the fused phase
+ * field in place (the phase field of the last step, i.e. of the state the
+ * last step started from) without exporting the populations. */
 int sym_neck_radius(sym_handle* h, double* rmin);
 /* FP64 sums over fluid nodes: out[0]=sum rho_R, [1]=sum rho_B, [2..4]=momentum. */
 int sym_mass_momentum(sym_handle* h, double out[5]);

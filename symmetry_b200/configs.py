@@ -121,32 +121,75 @@ def c3_thread(nx=256, ny=256, nz=512, steps=40000, storage="fp64", radius=24.0) 
     return Workload("c3_thread", p, "thread", gen, steps)
 
 
+def _c4_domain(rng, name, seed, storage, steps, wall_cita_deg=None, sphere_override=None) -> Workload:
+    """One domain of the batched-mix distribution (draw order fixed; the
+    sphere draw is consumed even when `sphere_override` decides it)."""
+    n = int(rng.integers(24, 65))
+    nz_raw = int(rng.integers(64, 385))
+    R = float(rng.uniform(4.0, 0.3 * n))
+    lam_ratio = float(rng.uniform(0.7, 2.0))
+    A = float(rng.uniform(2e-3, 1e-2))
+    tau = float(rng.uniform(0.6, 1.5))
+    sphere = bool(rng.integers(0, 2))
+    if sphere_override is not None:
+        sphere = bool(sphere_override)
+    lam = lam_ratio * 2.0 * math.pi * R
+    nwave = max(1, int(round(nz_raw / lam)))
+    nz = int(round(nwave * lam))
+    nz = max(nz, 16)
+    lam = nz / nwave
+    walls = wall_cita_deg is not None
+    p = config_params(n, n, nz, tau_r=tau, sigma=A, beta=0.7, rho0=1.0, storage=storage,
+                      par=1 if sphere else 0, rad=R / 2.0 if sphere else 0.0,
+                      rho_p_ratio=1.2, wall_x=walls, cita_deg=wall_cita_deg if walls else 90.0)
+    gen = dict(radius=R, amp=0.05, wavelength=lam, width=2.0, noise=1e-4, seed=seed)
+    parts = []
+    if sphere:
+        parts = [dict(center=[(n - 1) / 2.0, (n - 1) / 2.0, nz / 2.0], up=[0.0, 0.0, 0.0])]
+    return Workload(name, p, "thread", gen, steps, parts)
+
+
 def c4_manifest(n_domains=96, seed=4, storage="fp16", steps=3000) -> List[Workload]:
-    """Batched uneven Rayleigh-Plateau domains (frozen from default_rng(seed))."""
+    """Batched uneven Rayleigh-Plateau domains (frozen from default_rng(seed));
+    exactly half of them (the odd-numbered ones) carry the sphere."""
     rng = np.random.default_rng(seed)
-    out = []
-    for k in range(n_domains):
-        n = int(rng.integers(24, 65))
-        nz_raw = int(rng.integers(64, 385))
-        R = float(rng.uniform(4.0, 0.3 * n))
-        lam_ratio = float(rng.uniform(0.7, 2.0))
-        A = float(rng.uniform(2e-3, 1e-2))
-        tau = float(rng.uniform(0.6, 1.5))
-        sphere = bool(rng.integers(0, 2))
-        lam = lam_ratio * 2.0 * math.pi * R
-        nwave = max(1, int(round(nz_raw / lam)))
-        nz = int(round(nwave * lam))
-        nz = max(nz, 16)
-        lam = nz / nwave
-        p = config_params(n, n, nz, tau_r=tau, sigma=A, beta=0.7, rho0=1.0, storage=storage,
-                          par=1 if sphere else 0, rad=R / 2.0 if sphere else 0.0,
-                          rho_p_ratio=1.2)
-        gen = dict(radius=R, amp=0.05, wavelength=lam, width=2.0, noise=1e-4,
-                   seed=1004000 + k)
-        parts = []
-        if sphere:
-            parts = [dict(center=[(n - 1) / 2.0, (n - 1) / 2.0, nz / 2.0], up=[0.0, 0.0, 0.0])]
-        out.append(Workload(f"c4_{k:03d}", p, "thread", gen, steps, parts))
+    return [_c4_domain(rng, f"c4_{k:03d}", 1004000 + k, storage, steps, sphere_override=(k % 2 == 1))
+            for k in range(n_domains)]
+
+
+@dataclasses.dataclass
+class Job:
+    """One served job: its workload and its arrival time in seconds."""
+    workload: Workload
+    t_arrival: float
+    cita_deg: Optional[float]
+
+
+def c5_jobs(rate=20.0, duration=120.0, seed=5, storage="fp16", max_steps=50000) -> List[Job]:
+    """Open-loop Poisson arrivals (rate jobs/s for `duration` s), frozen from
+    default_rng(seed): 90% domains of the batched-mix distribution, 10%
+    128x128x512 threads with R=16 (the precision-study thread scaled down:
+    tau=0.7, A=8e-3, 2% perturbation over one 512 wavelength); each job has
+    wetting x walls with probability 0.3, contact angle uniform in [30,150]
+    degrees.  Seeds 1005000+j."""
+    rng = np.random.default_rng(seed)
+    out, t, j = [], 0.0, 0
+    while True:
+        t += float(rng.exponential(1.0 / rate))
+        if t >= duration:
+            break
+        big = bool(rng.random() < 0.1)
+        walls = bool(rng.random() < 0.3)
+        cita = float(rng.uniform(30.0, 150.0)) if walls else None
+        if big:
+            p = config_params(128, 128, 512, tau_r=0.7, sigma=8e-3, beta=0.7, rho0=1.0, storage=storage,
+                              wall_x=walls, cita_deg=cita if walls else 90.0)
+            gen = dict(radius=16.0, amp=0.02, wavelength=512.0, width=2.0, noise=1e-4, seed=1005000 + j)
+            w = Workload(f"c5_{j:04d}", p, "thread", gen, max_steps)
+        else:
+            w = _c4_domain(rng, f"c5_{j:04d}", 1005000 + j, storage, max_steps, cita)
+        out.append(Job(w, t, cita))
+        j += 1
     return out
 
 

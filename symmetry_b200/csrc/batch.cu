@@ -4,7 +4,9 @@
 //   k_phase_batch     calmacros of every domain in one launch (blocks map to
 //                     domains through a prefix sum of per-domain block counts);
 //   per-domain sparse particle coupling and pin fill (only domains with
-//                     solids; these are the small kernels of fast.cu);
+//                     solids; these are the small kernels of fast.cu), each
+//                     domain's chain on its own graph branch so the chains
+//                     of different domains run concurrently;
 //   k_collide_batch   one persistent launch (one CTA per SM slot) whose CTAs
 //                     take 32x8xX tiles of any domain from a work-tile table
 //                     through an atomic counter, largest tiles first, so
@@ -131,6 +133,11 @@ struct sym_batch {
   long long nblocks = 0;
   int* d_counter = nullptr;
   int grid = 0;
+  // fork/join of the per-domain sparse chains: one branch stream per solid
+  // domain (up to kBranches, then shared round robin)
+  std::vector<cudaStream_t> branch;
+  cudaEvent_t ev_fork = nullptr;
+  std::vector<cudaEvent_t> ev_join;
   cudaGraph_t graph[2] = {nullptr, nullptr};
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   bool built = false;
@@ -146,6 +153,7 @@ int berr(sym_batch* b, int code, const char* msg) {
 int bcuda(sym_batch* b, cudaError_t e, const char* what) {
   if (e == cudaSuccess) return SYM_OK;
   std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+  if (e == cudaErrorMemoryAllocation) (void)cudaGetLastError();   // not sticky: keep it out of later checks
   return berr(b, e == cudaErrorMemoryAllocation ? SYM_ERR_OOM : SYM_ERR_CUDA, m.c_str());
 }
 
@@ -188,25 +196,77 @@ DomainDesc make_desc(sym_handle* h, int cur, int pc) {
   return d;
 }
 
-template <typename S>
-int capture_step(sym_batch* b, int k) {
-  const int n = (int)b->doms.size();
-  k_phase_batch<S><<<(unsigned)b->nblocks, 256, 0, b->st>>>(b->d_desc[k], b->d_blk_off, n);
-  for (int i = 0; i < n; i++) {
-    sym_handle* h = b->doms[i];
-    if (!(h->dp.par > 0 || h->dp.wall_x)) continue;
-    const int cur = (b->built_cur[i] + k) & 1, pc = (b->built_pc[i] + k) & 1;
-    cudaStream_t saved = h->st;
-    h->st = b->st;   // the domain's sparse kernels join the batch graph
-    const int e = fast_enqueue_sparse(h, cur, pc);
-    h->st = saved;
-    if (e) return berr(b, e, h->err.c_str());
+constexpr int kBranches = 64;
+
+// create the branch streams and fork/join events for the solid domains
+int ensure_branches(sym_batch* b) {
+  int solid = 0;
+  for (sym_handle* h : b->doms) solid += (h->dp.par > 0 || h->dp.wall_x) ? 1 : 0;
+  const int want = std::min(solid, kBranches);
+  if (!b->ev_fork)
+    if (int e = bcuda(b, cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming), "fork event")) return e;
+  while ((int)b->branch.size() < want) {
+    cudaStream_t s = nullptr;
+    cudaEvent_t j = nullptr;
+    if (int e = bcuda(b, cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "branch stream")) return e;
+    if (int e = bcuda(b, cudaEventCreateWithFlags(&j, cudaEventDisableTiming), "join event")) {
+      cudaStreamDestroy(s);
+      return e;
+    }
+    b->branch.push_back(s);
+    b->ev_join.push_back(j);
   }
+  return SYM_OK;
+}
+
+// One batch step on b->st (captured into a graph, or eager when timing):
+// descriptor table k, domain i at buffer parity (built_cur[i] + k) & 1.
+// ev (optional, eager only): 4 events recorded before the phase launch, after
+// it, after the sparse chains have joined, and after the collide launch.
+template <typename S>
+int enqueue_batch_step(sym_batch* b, int k, cudaEvent_t* ev) {
+  const int n = (int)b->doms.size();
+  if (ev) cudaEventRecord(ev[0], b->st);
+  k_phase_batch<S><<<(unsigned)b->nblocks, 256, 0, b->st>>>(b->d_desc[k], b->d_blk_off, n);
+  if (ev) cudaEventRecord(ev[1], b->st);
+  if (!b->branch.empty()) {
+    cudaEventRecord(b->ev_fork, b->st);
+    std::vector<char> used(b->branch.size(), 0);
+    int j = 0;
+    for (int i = 0; i < n; i++) {
+      sym_handle* h = b->doms[i];
+      if (!(h->dp.par > 0 || h->dp.wall_x)) continue;
+      const int q = j++ % (int)b->branch.size();
+      if (!used[q]) {
+        cudaStreamWaitEvent(b->branch[q], b->ev_fork, 0);
+        used[q] = 1;
+      }
+      const int cur = (b->built_cur[i] + k) & 1, pc = (b->built_pc[i] + k) & 1;
+      cudaStream_t saved = h->st;
+      h->st = b->branch[q];   // the domain's sparse kernels go on its branch
+      const int e = fast_enqueue_sparse(h, cur, pc);
+      h->st = saved;
+      if (e) return berr(b, e, h->err.c_str());
+    }
+    for (size_t q = 0; q < b->branch.size(); q++)
+      if (used[q]) {
+        cudaEventRecord(b->ev_join[q], b->branch[q]);
+        cudaStreamWaitEvent(b->st, b->ev_join[q], 0);
+      }
+  }
+  if (ev) cudaEventRecord(ev[2], b->st);
   cudaMemsetAsync(b->d_counter + k, 0, sizeof(int), b->st);
   using R = typename Codec<S>::R;
   k_collide_batch<S><<<b->grid, kTPB, sizeof(Smem<R>), b->st>>>(b->d_desc[k], b->d_tiles, b->ntiles,
                                                                  b->d_counter + k);
+  if (ev) cudaEventRecord(ev[3], b->st);
   return bcuda(b, cudaGetLastError(), "batch step");
+}
+
+int enqueue_any(sym_batch* b, int k, cudaEvent_t* ev) {
+  return b->storage == SYM_STORE_FP64 ? enqueue_batch_step<double>(b, k, ev)
+       : b->storage == SYM_STORE_FP32 ? enqueue_batch_step<float>(b, k, ev)
+                                      : enqueue_batch_step<__half>(b, k, ev);
 }
 
 // (re)build the descriptor and tile tables and both step graphs
@@ -253,10 +313,10 @@ int build(sym_batch* b) {
   if (int e = bcuda(b, cudaMalloc(&b->d_tiles, sizeof(TileEntry) * std::max(1, b->ntiles)), "tiles")) return e;
   cudaMemcpyAsync(b->d_tiles, tiles.data(), sizeof(TileEntry) * b->ntiles, cudaMemcpyHostToDevice, b->st);
   if (int e = bcuda(b, cudaStreamSynchronize(b->st), "tables")) return e;
+  if (int e = ensure_branches(b)) return e;
   for (int k = 0; k < 2; k++) {
     if (int e = bcuda(b, cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal), "capture")) return e;
-    int e1 = b->storage == SYM_STORE_FP64 ? capture_step<double>(b, k)
-           : b->storage == SYM_STORE_FP32 ? capture_step<float>(b, k) : capture_step<__half>(b, k);
+    int e1 = enqueue_any(b, k, nullptr);
     cudaGraph_t g = nullptr;
     const cudaError_t e2 = cudaStreamEndCapture(b->st, &g);
     if (e1) { if (g) cudaGraphDestroy(g); return e1; }
@@ -295,6 +355,18 @@ int launch_steps(sym_batch* b, int nsteps) {
 }
 
 }  // namespace
+
+namespace symb200 {
+// asynchronous batch steps on the batch stream (the server overlaps batches
+// of different storage and enqueues its stop-rule reductions behind them)
+int batch_launch(sym_batch* b, int nsteps) {
+  cudaSetDevice(b->device);
+  if (stale(b))
+    if (int e = build(b)) return e;
+  return launch_steps(b, nsteps);
+}
+cudaStream_t batch_stream(sym_batch* b) { return b->st; }
+}  // namespace symb200
 
 extern "C" {
 
@@ -339,6 +411,9 @@ int sym_batch_destroy(sym_batch* b) {
   free_graphs(b);
   free_tables(b);
   if (b->d_counter) cudaFree(b->d_counter);
+  for (cudaStream_t s : b->branch) cudaStreamDestroy(s);
+  for (cudaEvent_t e : b->ev_join) cudaEventDestroy(e);
+  if (b->ev_fork) cudaEventDestroy(b->ev_fork);
   if (b->st) cudaStreamDestroy(b->st);
   delete b;
   return SYM_OK;
@@ -419,6 +494,67 @@ int sym_batch_autotune(sym_batch* b, int trial_steps, int* steps_taken) {
       if (cls(b->doms[i]->dp.nx) == c) sym_batch_set_xchunk(b, (int)i, bestx);
   }
   if (steps_taken) *steps_taken = taken;
+  return SYM_OK;
+}
+
+// nsteps eager (not graph) batch steps with CUDA events on the batch stream.
+// ms[0] = whole region, ms[1] = phase launches, ms[2] = per-domain sparse
+// chains (fork to join), ms[3] = collide launches (sums over the steps).
+int sym_batch_step_kernels(sym_batch* b, int nsteps, double* ms) {
+  if (!b || !ms || nsteps <= 0) return SYM_ERR_PARAM;
+  cudaSetDevice(b->device);
+  if (stale(b))
+    if (int e = build(b)) return e;
+  std::vector<cudaEvent_t> ev(4 * (size_t)nsteps + 2, nullptr);
+  int rc = SYM_OK;
+  for (auto& e : ev)
+    if (!rc) rc = bcuda(b, cudaEventCreate(&e), "event");
+  if (!rc) {
+    cudaEventRecord(ev[4 * nsteps], b->st);
+    for (int t = 0; t < nsteps && !rc; t++) {
+      const int k = b->steps_since_build & 1;
+      rc = enqueue_any(b, k, &ev[4 * t]);
+      b->steps_since_build++;
+      for (sym_handle* h : b->doms) {
+        h->fast.cur ^= 1;
+        h->fast.pc ^= 1;
+      }
+    }
+    cudaEventRecord(ev[4 * nsteps + 1], b->st);
+    if (!rc) rc = bcuda(b, cudaStreamSynchronize(b->st), "batch kernels");
+  }
+  if (!rc) {
+    float v = 0.f;
+    for (int k = 0; k < 4; k++) ms[k] = 0.0;
+    cudaEventElapsedTime(&v, ev[4 * nsteps], ev[4 * nsteps + 1]);
+    ms[0] = v;
+    for (int t = 0; t < nsteps; t++) {
+      cudaEventElapsedTime(&v, ev[4 * t], ev[4 * t + 1]); ms[1] += v;
+      cudaEventElapsedTime(&v, ev[4 * t + 1], ev[4 * t + 2]); ms[2] += v;
+      cudaEventElapsedTime(&v, ev[4 * t + 2], ev[4 * t + 3]); ms[3] += v;
+    }
+  }
+  for (auto& e : ev)
+    if (e) cudaEventDestroy(e);
+  return rc;
+}
+
+// Kernel launches in one captured batch step (kernel nodes of the graph).
+int sym_batch_kernels_per_step(sym_batch* b, int* kernels) {
+  if (!b || !kernels) return SYM_ERR_PARAM;
+  cudaSetDevice(b->device);
+  if (stale(b))
+    if (int e = build(b)) return e;
+  size_t n = 0;
+  if (int e = bcuda(b, cudaGraphGetNodes(b->graph[0], nullptr, &n), "graph nodes")) return e;
+  std::vector<cudaGraphNode_t> nodes(n);
+  if (int e = bcuda(b, cudaGraphGetNodes(b->graph[0], nodes.data(), &n), "graph nodes")) return e;
+  int cnt = 0;
+  for (size_t i = 0; i < n; i++) {
+    cudaGraphNodeType t;
+    if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) cnt++;
+  }
+  *kernels = cnt;
   return SYM_OK;
 }
 

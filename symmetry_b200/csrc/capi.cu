@@ -28,6 +28,34 @@ int check_cuda(sym_handle* h, cudaError_t e, const char* what) {
                    cudaGetErrorString(e));
 }
 
+int dev_carve(sym_handle* h, void** p, size_t bytes) {
+  const size_t b = (bytes + 255) / 256 * 256;
+  *p = nullptr;
+  if (h->planning) {
+    h->slab_size += b;
+    return SYM_OK;
+  }
+  if (h->slab && h->slab_used + b <= h->slab_size) {
+    *p = h->slab + h->slab_used;
+    h->slab_used += b;
+  } else {
+    const cudaError_t e = cudaMalloc(p, b);
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();   // a failed allocation must not surface in a later launch check
+      *p = nullptr;
+      return check_cuda(h, e, "cudaMalloc");
+    }
+  }
+  h->bytes += b;
+  return check_cuda(h, cudaMemsetAsync(*p, 0, b, h->st), "memset");
+}
+
+void dev_release(sym_handle* h, void* p) {
+  if (!p) return;
+  if (h->slab && static_cast<char*>(p) >= h->slab && static_cast<char*>(p) < h->slab + h->slab_size) return;
+  cudaFree(p);
+}
+
 void fill_devparams(const sym_params& p, DevParams& d) {
   d.nx = p.nx; d.ny = p.ny; d.nz = p.nz;
   d.N = (long long)p.nx * p.ny * p.nz;
@@ -52,6 +80,8 @@ void fill_devparams(const sym_params& p, DevParams& d) {
   d.inertia = p.inertia > 0 ? p.inertia : 2.0 / 5.0 * d.mass * (p.rad * p.rad);
   d.fg = p.fg; d.alpha = p.alpha;
   d.evap = p.evap_lim > 0 ? p.evap_lim : 1.0e-8;
+  d.inu_r = p.nu_r > 0 ? 1.0 / p.nu_r : 0.0;
+  d.inu_b = p.nu_b > 0 ? 1.0 / p.nu_b : 0.0;
 }
 
 }  // namespace symb200
@@ -60,10 +90,10 @@ namespace {
 
 template <typename T>
 int dalloc(sym_handle* h, T** p, size_t n) {
-  cudaError_t e = cudaMalloc((void**)p, sizeof(T) * n);
-  if (e != cudaSuccess) return check_cuda(h, e, "cudaMalloc");
-  h->bytes += sizeof(T) * n;
-  return check_cuda(h, cudaMemsetAsync(*p, 0, sizeof(T) * n, h->st), "memset");
+  void* v = nullptr;
+  const int e = dev_carve(h, &v, sizeof(T) * n);
+  *p = static_cast<T*>(v);
+  return e;
 }
 
 size_t reduction_len(const sym_params& p) {
@@ -75,6 +105,7 @@ size_t reduction_len(const sym_params& p) {
     const double e = std::ceil(2.0 * (p.rad + 3.0)) + 2.0;
     const size_t box = (size_t)(e * e * e);
     n = std::max(n, ((box + 255) / 256) * 6 * (size_t)p.par + 16);
+    n = std::max(n, (size_t)32 * 7 * p.par + 16);   // capillary partial sums
   }
   return n;
 }
@@ -178,6 +209,40 @@ int canonical_steps(sym_handle* h, int nsteps) {
   return check_cuda(h, cudaStreamSynchronize(h->st), "step");
 }
 
+// Every array a new handle holds, in one fixed order; with h->planning set it
+// only sums the sizes.
+int alloc_state(sym_handle* h) {
+  const sym_params& p = h->p;
+  const size_t N = h->N;
+  int e = SYM_OK;
+  // ri, bi always; fi, ffi and the streaming/transfer temporary ft only where
+  // the mode needs them up front (REFERENCE subroutines, particle coupling),
+  // otherwise on the first call that uses them (ensure_full)
+  double** pops[2] = {&h->ri, &h->bi};
+  for (auto pp : pops)
+    if (!e) e = dalloc(h, pp, 19 * N);
+  if (!e && (p.mode == SYM_MODE_REFERENCE || p.par > 0)) e = ensure_full(h);
+  double** sc[13] = {&h->rho, &h->ux, &h->uy, &h->uz, &h->rhoN, &h->rhoR, &h->rhoB,
+                     &h->nx, &h->ny, &h->nz, &h->gx, &h->gy, &h->gz};
+  for (auto pp : sc)
+    if (!e) e = dalloc(h, pp, N);
+  int32_t** ms[6] = {&h->flag, &h->walls, &h->walls_old, &h->walls_all, &h->pin, &h->pout};
+  for (auto pp : ms)
+    if (!e) e = dalloc(h, pp, N);
+  if (!e) e = dalloc(h, &h->dpart, 1);
+  const size_t NL = (size_t)h->dp.la_num * h->dp.par;
+  if (NL) {
+    double** la[8] = {&h->lax, &h->lay, &h->laz, &h->larhon, &h->lanx, &h->lany, &h->lanz, &h->lads};
+    for (auto pp : la)
+      if (!e) e = dalloc(h, pp, NL);
+    if (!e) e = dalloc(h, &h->laflag, NL);
+  }
+  h->red_len = reduction_len(p);
+  if (!e) e = dalloc(h, &h->red, h->red_len);
+  if (!e && p.mode == SYM_MODE_CONFIG) e = fast_alloc(h);
+  return e;
+}
+
 }  // namespace
 
 extern "C" {
@@ -236,18 +301,14 @@ int sym_params_check(const sym_params* p, char* msg, size_t msg_len) {
 
 int sym_footprint(const sym_params* p, size_t* bytes) {
   if (!p || !bytes) return SYM_ERR_PARAM;
-  const size_t N = (size_t)p->nx * p->ny * p->nz;
-  const bool full = p->mode == SYM_MODE_REFERENCE || p->par > 0;
-  size_t b = (full ? 5 : 2) * 19 * N * 8 + 13 * N * 8 + 6 * N * 4 + reduction_len(*p) * 8 + sizeof(sym_particles);
-  const int lam = p->la_m > 0 ? p->la_m : (p->alpha > 0 ? (int)(2.0 * M_PI / p->alpha) : 0);
-  const int lan = p->la_n > 0 ? p->la_n : (p->alpha > 0 ? (int)(M_PI / p->alpha) : 0);
-  b += (size_t)p->par * lam * (lan + 1) * (8 * 8 + 4);
-  if (p->mode == SYM_MODE_CONFIG) {
-    const size_t s = p->storage == SYM_STORE_FP64 ? 8 : (p->storage == SYM_STORE_FP32 ? 4 : 2);
-    const size_t pad = (size_t)(p->nx + 4) * (p->ny + 4) * ((p->nz + 4 + 3) / 4 * 4);
-    b += 2 * 38 * N * s + 2 * pad * (p->storage == SYM_STORE_FP64 ? 8 : 4);
-  }
-  *bytes = b;
+  if (int e = sym_params_check(p, nullptr, 0)) return e;
+  sym_handle h;   // planning pass: sizes only, no device calls
+  h.p = *p;
+  fill_devparams(*p, h.dp);
+  h.N = (size_t)h.dp.N;
+  h.planning = true;
+  if (int e = alloc_state(&h)) return e;
+  *bytes = h.slab_size;
   return SYM_OK;
 }
 
@@ -264,34 +325,21 @@ int sym_create(const sym_params* p, int device, sym_handle** out) {
   h->device = device;
   fill_devparams(*p, h->dp);
   h->N = (size_t)h->dp.N;
-  int e = check_cuda(h, cudaSetDevice(device), "cudaSetDevice");
+  h->planning = true;
+  int e = alloc_state(h);
+  h->planning = false;
+  h->bytes = 0;
+  if (!e) e = check_cuda(h, cudaSetDevice(device), "cudaSetDevice");
   if (!e) e = check_cuda(h, cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking), "stream");
-  const size_t N = h->N;
-  // ri, bi always; fi, ffi and the streaming/transfer temporary ft only where
-  // the mode needs them up front (REFERENCE subroutines, particle coupling),
-  // otherwise on the first call that uses them (ensure_full)
-  double** pops[2] = {&h->ri, &h->bi};
-  for (auto pp : pops)
-    if (!e) e = dalloc(h, pp, 19 * N);
-  if (!e && (p->mode == SYM_MODE_REFERENCE || p->par > 0)) e = ensure_full(h);
-  double** sc[13] = {&h->rho, &h->ux, &h->uy, &h->uz, &h->rhoN, &h->rhoR, &h->rhoB,
-                     &h->nx, &h->ny, &h->nz, &h->gx, &h->gy, &h->gz};
-  for (auto pp : sc)
-    if (!e) e = dalloc(h, pp, N);
-  int32_t** ms[6] = {&h->flag, &h->walls, &h->walls_old, &h->walls_all, &h->pin, &h->pout};
-  for (auto pp : ms)
-    if (!e) e = dalloc(h, pp, N);
-  if (!e) e = dalloc(h, &h->dpart, 1);
-  const size_t NL = (size_t)h->dp.la_num * h->dp.par;
-  if (NL) {
-    double** la[8] = {&h->lax, &h->lay, &h->laz, &h->larhon, &h->lanx, &h->lany, &h->lanz, &h->lads};
-    for (auto pp : la)
-      if (!e) e = dalloc(h, pp, NL);
-    if (!e) e = dalloc(h, &h->laflag, NL);
+  if (!e) {
+    const cudaError_t ce = cudaMalloc((void**)&h->slab, h->slab_size);
+    if (ce != cudaSuccess) {
+      (void)cudaGetLastError();
+      h->slab = nullptr;
+      e = check_cuda(h, ce, "device state");
+    }
   }
-  h->red_len = reduction_len(*p);
-  if (!e) e = dalloc(h, &h->red, h->red_len);
-  if (!e && p->mode == SYM_MODE_CONFIG) e = fast_alloc(h);
+  if (!e) e = alloc_state(h);
   if (!e) e = check_cuda(h, cudaStreamSynchronize(h->st), "create");
   if (e) {
     fprintf(stderr, "sym_create: %s\n", h->err.c_str());
@@ -313,8 +361,8 @@ int sym_destroy(sym_handle* h) {
                   h->nx, h->ny, h->nz, h->gx, h->gy, h->gz, h->flag, h->walls, h->walls_old, h->walls_all,
                   h->pin, h->pout, h->dpart, h->lax, h->lay, h->laz, h->larhon, h->lanx, h->lany, h->lanz,
                   h->lads, h->laflag, h->red};
-  for (void* q : ptrs)
-    if (q) cudaFree(q);
+  for (void* q : ptrs) dev_release(h, q);
+  if (h->slab) cudaFree(h->slab);
   if (h->st) cudaStreamDestroy(h->st);
   delete h;
   return SYM_OK;
@@ -459,27 +507,30 @@ int sym_init_slab(sym_handle* h, double z0, double z1, double width, double nois
 }
 
 // ---- the reference's subroutines -----------------------------------------------
-#define SYM_SUBROUTINE(name, call)                                     \
+// `full`: the subroutine reads or writes fi, ffi or the temporary ft, which
+// a CONFIG handle without particles allocates on first use
+#define SYM_SUBROUTINE(name, call, full)                               \
   int name(sym_handle* h) {                                            \
     if (int e = guard(h)) return e;                                    \
-    if (int e = ensure_full(h)) return e;                              \
+    if (full)                                                          \
+      if (int e = ensure_full(h)) return e;                            \
     if (int e = canonical(h)) return e;                                \
     if (int e = call) return e;                                        \
     return check_cuda(h, cudaStreamSynchronize(h->st), #name);         \
   }
-SYM_SUBROUTINE(sym_set_walls, part_set_walls(h))
-SYM_SUBROUTINE(sym_calmacros, ref_calmacros(h))
-SYM_SUBROUTINE(sym_derivatives, ref_derivatives(h))
-SYM_SUBROUTINE(sym_collision, ref_collision(h))
-SYM_SUBROUTINE(sym_recolor, ref_recolor(h))
-SYM_SUBROUTINE(sym_boundary, ref_boundary(h))
-SYM_SUBROUTINE(sym_curve, ref_curve(h))
-SYM_SUBROUTINE(sym_lagrange_points, part_lagrange_points(h))
-SYM_SUBROUTINE(sym_capillary_force2, part_capillary_force2(h))
-SYM_SUBROUTINE(sym_momentum, part_momentum(h))
-SYM_SUBROUTINE(sym_repulsive, part_repulsive(h))
-SYM_SUBROUTINE(sym_movement, part_movement(h))
-SYM_SUBROUTINE(sym_refilling, part_refilling(h))
+SYM_SUBROUTINE(sym_set_walls, part_set_walls(h), false)
+SYM_SUBROUTINE(sym_calmacros, ref_calmacros(h), true)
+SYM_SUBROUTINE(sym_derivatives, ref_derivatives(h), false)
+SYM_SUBROUTINE(sym_collision, ref_collision(h), true)
+SYM_SUBROUTINE(sym_recolor, ref_recolor(h), true)
+SYM_SUBROUTINE(sym_boundary, ref_boundary(h), true)
+SYM_SUBROUTINE(sym_curve, ref_curve(h), true)
+SYM_SUBROUTINE(sym_lagrange_points, part_lagrange_points(h), false)
+SYM_SUBROUTINE(sym_capillary_force2, part_capillary_force2(h), false)
+SYM_SUBROUTINE(sym_momentum, part_momentum(h), true)
+SYM_SUBROUTINE(sym_repulsive, part_repulsive(h), false)
+SYM_SUBROUTINE(sym_movement, part_movement(h), false)
+SYM_SUBROUTINE(sym_refilling, part_refilling(h), true)
 #undef SYM_SUBROUTINE
 
 int sym_streaming(sym_handle* h, int which) {
@@ -550,7 +601,19 @@ int sym_output3(sym_handle* h, double* hmin, int32_t* y0) {
 int sym_neck_radius(sym_handle* h, double* rmin) {
   if (int e = guard(h)) return e;
   if (!rmin) return set_error(h, SYM_ERR_PARAM, "null output");
-  if (int e = canonical(h)) return e;
+  if (h->fast.valid) {
+    // the fused phase field is the rho_N an export would produce: reduce it
+    // in place instead of exporting the populations
+    const int nz = h->dp.nz;
+    if (int e = fast_neck_planes(h, h->red, h->st)) return e;
+    std::vector<double> a(nz);
+    cudaMemcpyAsync(a.data(), h->red, sizeof(double) * nz, cudaMemcpyDeviceToHost, h->st);
+    if (int e = check_cuda(h, cudaStreamSynchronize(h->st), "neck_radius")) return e;
+    double mn = 1e300;
+    for (int z = 0; z < nz; z++) mn = std::fmin(mn, std::sqrt(a[z] / M_PI));
+    *rmin = mn;
+    return SYM_OK;
+  }
   return ref_neck_radius(h, rmin);
 }
 int sym_mass_momentum(sym_handle* h, double out[5]) {

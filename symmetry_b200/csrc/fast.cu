@@ -145,6 +145,31 @@ int set_smem_attr(sym_handle* h) {
   return check_cuda(h, e, "smem attribute");
 }
 
+// Stop-rule reduction on the fused phase field: per z plane, the sum over
+// fluid nodes of (1+phi)/2 (the red area of the plane), one block per plane,
+// in a fixed order (deterministic).  phi on solid nodes holds the pin fill
+// and is skipped.
+template <typename R>
+__global__ void __launch_bounds__(256) k_neck_planes(DevParams P, Pad pd, const R* __restrict__ phi,
+                                                     const int32_t* __restrict__ walls_all, double* out) {
+  __shared__ double sh[256];
+  const int z = blockIdx.x;
+  double s = 0.0;
+  const int nxy = P.nx * P.ny;
+  for (int t = threadIdx.x; t < nxy; t += 256) {
+    const int x = t / P.ny, y = t - x * P.ny;
+    const long long L = (long long)z + (long long)P.nz * ((long long)y + (long long)P.ny * x);
+    if (walls_all[L] <= 0) s += 0.5 * (1.0 + (double)phi[pd.idx(x, y, z)]);
+  }
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int k = 128; k > 0; k >>= 1) {
+    if ((int)threadIdx.x < k) sh[threadIdx.x] += sh[threadIdx.x + k];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[z] = sh[0];
+}
+
 int enqueue_sparse_any(sym_handle* h, int cur, int pc) {
   switch (h->fast.storage) {
     case SYM_STORE_FP64: return enqueue_sparse<double>(h, cur, pc);
@@ -171,34 +196,29 @@ int fast_alloc(sym_handle* h) {
   F.storage = h->p.storage;
   const size_t s = F.storage == SYM_STORE_FP64 ? 8 : (F.storage == SYM_STORE_FP32 ? 4 : 2);
   const size_t popb = 38 * h->N * s;
-  for (int k = 0; k < 2; k++) {
-    if (cudaMalloc(&F.pop[k], popb) != cudaSuccess) return set_error(h, SYM_ERR_OOM, "fast populations");
-    F.bytes += popb;
-  }
+  const size_t before = h->bytes;
+  for (int k = 0; k < 2; k++)
+    if (int e = dev_carve(h, &F.pop[k], popb)) return e;
   const Pad pd = make_pad(h->dp);
   for (int k = 0; k < 2; k++) {
     if (F.storage == SYM_STORE_FP64) {
-      if (cudaMalloc(&F.phi[k], sizeof(double) * pd.size()) != cudaSuccess) return set_error(h, SYM_ERR_OOM, "phi");
-      cudaMemsetAsync(F.phi[k], 0, sizeof(double) * pd.size(), h->st);
-      F.bytes += sizeof(double) * pd.size();
+      if (int e = dev_carve(h, (void**)&F.phi[k], sizeof(double) * pd.size())) return e;
     } else {
-      if (cudaMalloc(&F.phif[k], sizeof(float) * pd.size()) != cudaSuccess) return set_error(h, SYM_ERR_OOM, "phi");
-      cudaMemsetAsync(F.phif[k], 0, sizeof(float) * pd.size(), h->st);
-      F.bytes += sizeof(float) * pd.size();
+      if (int e = dev_carve(h, (void**)&F.phif[k], sizeof(float) * pd.size())) return e;
     }
   }
-  h->bytes += F.bytes;
-  int e = F.storage == SYM_STORE_FP64 ? set_smem_attr<double>(h)
-        : F.storage == SYM_STORE_FP32 ? set_smem_attr<float>(h) : set_smem_attr<__half>(h);
-  return e;
+  if (h->planning) return SYM_OK;
+  F.bytes = h->bytes - before;
+  return F.storage == SYM_STORE_FP64 ? set_smem_attr<double>(h)
+       : F.storage == SYM_STORE_FP32 ? set_smem_attr<float>(h) : set_smem_attr<__half>(h);
 }
 
 void fast_free(sym_handle* h) {
   FastState& F = h->fast;
   for (int k = 0; k < 2; k++) {
-    if (F.pop[k]) cudaFree(F.pop[k]);
-    if (F.phi[k]) cudaFree(F.phi[k]);
-    if (F.phif[k]) cudaFree(F.phif[k]);
+    dev_release(h, F.pop[k]);
+    dev_release(h, F.phi[k]);
+    dev_release(h, F.phif[k]);
     if (F.gexec[k]) cudaGraphExecDestroy(F.gexec[k]);
     if (F.graph[k]) cudaGraphDestroy(F.graph[k]);
     F.pop[k] = nullptr; F.phi[k] = nullptr; F.phif[k] = nullptr; F.gexec[k] = nullptr; F.graph[k] = nullptr;
@@ -309,6 +329,25 @@ int fast_step_timed(sym_handle* h, int nsteps, double ms[4]) {
   }
   for (auto& e : ev) cudaEventDestroy(e);
   return rc;
+}
+
+}  // namespace symb200
+
+namespace symb200 {
+
+// Per-plane red area of the phase field written by the last fused step
+// (phi of the populations that step started from), enqueued on `st` into
+// device memory `out` (nz doubles).  r_eq(z) = sqrt(out[z] / pi).
+int fast_neck_planes(sym_handle* h, double* out, cudaStream_t st) {
+  FastState& F = h->fast;
+  if (!F.valid) return set_error(h, SYM_ERR_STATE, "neck planes: the fused state is not current");
+  const DevParams& P = h->dp;
+  const Pad pd = make_pad(P);
+  if (F.storage == SYM_STORE_FP64)
+    k_neck_planes<double><<<P.nz, 256, 0, st>>>(P, pd, F.phi[1 - F.pc], h->walls_all, out);
+  else
+    k_neck_planes<float><<<P.nz, 256, 0, st>>>(P, pd, F.phif[1 - F.pc], h->walls_all, out);
+  return check_cuda(h, cudaGetLastError(), "neck planes");
 }
 
 }  // namespace symb200

@@ -46,11 +46,16 @@ __device__ __forceinline__ void phi_store(const DevParams& P, const Pad& pd, R* 
 }
 
 // ---- population storage codecs --------------------------------------------------
-// Slot 0 and slot 1 of each velocity hold (r, b) for FP64/FP32; for the
-// 16-bit storage they hold q = f/(w rho0) - 1 (FP16 shifted storage) and the
-// colour fraction c = r/f (16-bit fixed point).
-// Indices are 32-bit element offsets (the fused path requires 38*N < 2^32).
-// load takes rho0, store takes 1/rho0 (only the FP16 codec uses them).
+// Each velocity i holds an array of N slot pairs, pair index i*N + L: one
+// aligned 2-slot load or store per velocity (8/16-byte pairs, 4-byte for the
+// 16-bit storage), so a warp moves whole 128-byte lines per instruction.
+// FP64 / FP32: the pair is (r, b).  16-bit storage: the low half holds
+// q = f/(w rho0) - 1 in FP16 (the deviation of the total population from its
+// rest equilibrium w rho0), the high half the colour fraction c = r/f as
+// 16-bit fixed point k = 16384 + 32768 c over c in [-0.5, 1.5) (step 3.05e-5;
+// the pure phases c = 0 and c = 1 are the exact codes 16384 and 49152).
+// Indices are 32-bit pair offsets (the fused path requires 38*N < 2^32).
+// load takes rho0, store takes 1/rho0 (only the 16-bit codec uses them).
 template <typename S>
 struct Codec;
 template <>
@@ -58,13 +63,13 @@ struct Codec<double> {
   using R = double;
   template <int I>
   __device__ __forceinline__ static void load(const double* __restrict__ p, unsigned N, unsigned L, R, R& r, R& b) {
-    r = p[I * N + L];
-    b = p[(19 + I) * N + L];
+    const double2 v = reinterpret_cast<const double2*>(p)[I * N + L];
+    r = v.x;
+    b = v.y;
   }
   template <int I>
   __device__ __forceinline__ static void store(double* p, unsigned N, unsigned L, R, R r, R f) {
-    p[I * N + L] = r;
-    p[(19 + I) * N + L] = f - r;
+    reinterpret_cast<double2*>(p)[I * N + L] = make_double2(r, f - r);
   }
 };
 template <>
@@ -72,30 +77,26 @@ struct Codec<float> {
   using R = float;
   template <int I>
   __device__ __forceinline__ static void load(const float* __restrict__ p, unsigned N, unsigned L, R, R& r, R& b) {
-    r = p[I * N + L];
-    b = p[(19 + I) * N + L];
+    const float2 v = reinterpret_cast<const float2*>(p)[I * N + L];
+    r = v.x;
+    b = v.y;
   }
   template <int I>
   __device__ __forceinline__ static void store(float* p, unsigned N, unsigned L, R, R r, R f) {
-    p[I * N + L] = r;
-    p[(19 + I) * N + L] = f - r;
+    reinterpret_cast<float2*>(p)[I * N + L] = make_float2(r, f - r);
   }
 };
-// FP16 shifted storage: slot 0 holds q = f/(w rho0) - 1 as FP16 (the deviation
-// of the total population from its rest equilibrium w rho0); slot 1 holds the
-// colour fraction c = r/f as 16-bit fixed point k = 16384 + 32768 c over
-// c in [-0.5, 1.5) (step 3.05e-5; the pure phases c = 0 and c = 1 are the
-// exact codes 16384 and 49152).
 template <>
 struct Codec<__half> {
   using R = float;
   template <int I>
   __device__ __forceinline__ static void load(const __half* __restrict__ p, unsigned N, unsigned L, R rho0, R& r,
                                               R& b) {
-    const R q = __half2float(p[I * N + L]);
-    const unsigned short k = reinterpret_cast<const unsigned short*>(p)[(19 + I) * N + L];
-    const R c = fmaf((R)k, 1.0f / 32768.0f, -0.5f);
-    const R f = (R(W(I)) * rho0) * (R(1) + q);
+    const unsigned w = reinterpret_cast<const unsigned*>(p)[I * N + L];
+    const R q = __half2float(__ushort_as_half((unsigned short)(w & 0xffffu)));
+    const R c = fmaf((R)(w >> 16), 1.0f / 32768.0f, -0.5f);
+    const R wr = R(W(I)) * rho0;
+    const R f = fmaf(wr, q, wr);
     r = f * c;
     b = f - r;
   }
@@ -104,8 +105,9 @@ struct Codec<__half> {
     const R q = f * (R(1.0 / W(I)) * irho0) - R(1);
     const R c = __fdividef(r, f);
     const R kf = fminf(fmaxf(fmaf(c, 32768.0f, 16384.0f), 0.0f), 65535.0f);
-    p[I * N + L] = __float2half_rn(q);
-    reinterpret_cast<unsigned short*>(p)[(19 + I) * N + L] = (unsigned short)__float2uint_rn(kf);
+    const unsigned lo = __half_as_ushort(__float2half_rn(q));
+    const unsigned hi = __float2uint_rn(kf);
+    reinterpret_cast<unsigned*>(p)[I * N + L] = lo | (hi << 16);
   }
 };
 
@@ -258,7 +260,7 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
     if (x + 1 < xb) {
       // bring the next plane's populations toward L2 while this plane computes
 #pragma unroll
-      for (int i = 0; i < 38; i++) asm volatile("prefetch.global.L2 [%0];" ::"l"(pin_ + (i * N + L + sx)));
+      for (int i = 0; i < 19; i++) asm volatile("prefetch.global.L2 [%0];" ::"l"(pin_ + 2 * (i * N + L + sx)));
     }
     int pp = 0;
     if (SOLID) {
@@ -284,7 +286,8 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
       if (CY(i)) uy = uy + f[i] * R(CY(i));
       if (CZ(i)) uz = uz + f[i] * R(CZ(i));
     }
-    ux = ux / rho; uy = uy / rho; uz = uz / rho;
+    const R irho = R(1) / rho;
+    ux = ux * irho; uy = uy * irho; uz = uz * irho;
     const int s1 = x % 4;
     const R nx = sm.n[s1][0][ty + 1][tz + 1], ny = sm.n[s1][1][ty + 1][tz + 1], nz = sm.n[s1][2][ty + 1][tz + 1];
     const R fn = sm.n[s1][3][ty + 1][tz + 1];
@@ -315,17 +318,21 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
     fx = fx + rho * R(P.body[0]);
     fy = fy + rho * R(P.body[1]);
     fz = fz + rho * R(P.body[2]);
-    ux = ux + R(0.5) * fx / rho;
-    uy = uy + R(0.5) * fy / rho;
-    uz = uz + R(0.5) * fz / rho;
-    mrt_collide<R>(P, f, rho, ux, uy, uz, fx, fy, fz, rhoN);
-    if (SOLID && pp >= 1) {
+    const R hirho = R(0.5) * irho;
+    ux = ux + fx * hirho;
+    uy = uy + fy * hirho;
+    uz = uz + fz * hirho;
+    mrt_collide_pairs<R>(P, f, rho, ux, uy, uz, fx, fy, fz, rhoN);
+    // post-collision populations for the momentum exchange (:1241-1243), read
+    // only next to particles (pout = particle id); wall planes (ids > par)
+    // need none, and a handle without particles holds no ffi array
+    if (SOLID && pp >= 1 && pp <= P.par) {
 #pragma unroll
       for (int i = 0; i < 19; i++) ffi[(size_t)i * N + L] = (double)f[i];
     }
     // Latva-Kokko recolouring (:712-726) and push streaming with bounce-back
-    const R ratio = sr / rho;
-    const R coef = sr * sb / rho * R(P.beta);
+    const R ratio = sr * irho;
+    const R coef = sr * sb * irho * R(P.beta);
     const bool rzero = sr <= evap, bzero = sb <= evap;
     // neighbour offsets with the periodic wrap folded in (one select per face)
     const int oxp = (x == P.nx - 1) ? -(P.nx - 1) * sx : sx, oxm = (x == 0) ? (P.nx - 1) * sx : -sx;

@@ -5,6 +5,7 @@
 // adds/multiplies with no zero terms and no memory operands.
 #pragma once
 #include <cstdint>
+#include <utility>
 #include <cuda_runtime.h>
 #include "../../include/symmetry.h"
 
@@ -93,6 +94,7 @@ struct DevParams {
   double sigma, beta, cita;
   double body[3];
   double rad, mass, inertia, fg, alpha, evap;
+  double inu_r, inu_b;     // 1/nu_r, 1/nu_b (fused path)
 };
 
 template <typename T>
@@ -115,18 +117,20 @@ __device__ __forceinline__ double disp(const DevParams& P, double c, double cen,
 }
 
 // equilf (Source1.f90:397-450): equilibrium moments and Guo forcing moments.
-template <typename R>
+// EXACT keeps the reference's divisions by 1.5; the fused path multiplies by
+// 2/3 instead (same value up to one rounding).
+template <typename R, bool EXACT = true>
 __device__ __forceinline__ void equilf(R meq[19], R fk[19], R rho, R ux, R uy, R uz, R fx, R fy, R fz) {
   const R usqr = ux * ux + uy * uy + uz * uz;
   meq[0] = R(1);
   meq[1] = R(19) * usqr - R(11);
   meq[2] = R(3) - R(5.5) * usqr;
   meq[3] = ux;
-  meq[4] = -ux / R(1.5);
+  meq[4] = EXACT ? -ux / R(1.5) : ux * R(-2.0 / 3.0);
   meq[5] = uy;
-  meq[6] = -uy / R(1.5);
+  meq[6] = EXACT ? -uy / R(1.5) : uy * R(-2.0 / 3.0);
   meq[7] = uz;
-  meq[8] = -uz / R(1.5);
+  meq[8] = EXACT ? -uz / R(1.5) : uz * R(-2.0 / 3.0);
   meq[9] = R(3) * ux * ux - usqr;
   meq[10] = R(-0.5) * (R(3) * ux * ux - usqr);
   meq[11] = uy * uy - uz * uz;
@@ -144,11 +148,11 @@ __device__ __forceinline__ void equilf(R meq[19], R fk[19], R rho, R ux, R uy, R
   fk[1] = R(38) * uf;
   fk[2] = R(-11) * uf;
   fk[3] = fx;
-  fk[4] = -fx / R(1.5);
+  fk[4] = EXACT ? -fx / R(1.5) : fx * R(-2.0 / 3.0);
   fk[5] = fy;
-  fk[6] = -fy / R(1.5);
+  fk[6] = EXACT ? -fy / R(1.5) : fy * R(-2.0 / 3.0);
   fk[7] = fz;
-  fk[8] = -fz / R(1.5);
+  fk[8] = EXACT ? -fz / R(1.5) : fz * R(-2.0 / 3.0);
   fk[9] = R(6) * ux * fx - R(2) * uf;
   fk[10] = -(R(3) * ux * fx - uf);
   fk[11] = R(2) * (uy * fy - uz * fz);
@@ -176,6 +180,23 @@ __device__ __forceinline__ void node_rates(const DevParams& P, R rhoN, R& su, R&
   else if (rhoN >= R(1)) nu = R(P.nu_r);
   else nu = R(2) / ((R(1) + rhoN) / R(P.nu_r) + (R(1) - rhoN) / R(P.nu_b));
   su = R(1) / (R(3) * nu + R(0.5));
+  const R sq_ = R(8) * (R(2) - su) / (R(8) - su);
+  se = P.s_e > 0 ? R(P.s_e) : su;
+  seps = P.s_eps > 0 ? R(P.s_eps) : su;
+  sq = P.s_q > 0 ? R(P.s_q) : sq_;
+  spi = P.s_pi > 0 ? R(P.s_pi) : su;
+  sm = P.s_m > 0 ? R(P.s_m) : sq_;
+}
+
+// The same rates with two divisions (fused path): with phi clamped to
+// [-1, 1] and D = (1+phi)/nu_r + (1-phi)/nu_b, nu = 2/D gives the branches
+// of the reference at the ends, so su = 1/(3 nu + 1/2) = 2D/(12 + D).
+template <typename R>
+__device__ __forceinline__ void node_rates_fast(const DevParams& P, R rhoN, R& su, R& se, R& seps, R& sq, R& spi,
+                                                R& sm) {
+  const R ph = fmin(fmax(rhoN, R(-1)), R(1));
+  const R D = (R(1) + ph) * R(P.inu_r) + (R(1) - ph) * R(P.inu_b);
+  su = R(2) * D / (R(12) + D);
   const R sq_ = R(8) * (R(2) - su) / (R(8) - su);
   se = P.s_e > 0 ? R(P.s_e) : su;
   seps = P.s_eps > 0 ? R(P.s_eps) : su;
@@ -220,6 +241,89 @@ __device__ __forceinline__ void mrt_collide(const DevParams& P, R f[19], R rho, 
     }
     f[r] = acc;
   }
+}
+
+// The same collision in the opposite-pair basis (fused path).  Row r of M is
+// even (M(r,opc(c)) = M(r,c)) or odd (= -M(r,c)) under velocity reversal, so
+// with p_k = f_i + f_opc(i) and q_k = f_i - f_opc(i) over the 9 pairs the even
+// moments need only p (and f_0) and the odd ones only q; back-transformed,
+// f_i = E_i + O_i and f_opc(i) = E_i - O_i with E (O) the sum over even (odd)
+// rows.  Half the multiply-adds of the dense form; the result differs from it
+// only by rounding order.
+__host__ __device__ __forceinline__ constexpr int PREP(int k) {   // pair representatives, k = 0..8
+  constexpr int a[9] = {1, 3, 5, 7, 8, 11, 12, 15, 16};
+  return a[k];
+}
+__host__ __device__ __forceinline__ constexpr bool MEVEN(int r) {
+  for (int c = 0; c < 19; c++)
+    if (MROW(r, OPC(c)) != MROW(r, c)) return false;
+  return true;
+}
+
+template <int... Is, typename F>
+__device__ __forceinline__ void static_for_impl(F&& f, std::integer_sequence<int, Is...>) {
+  (f(std::integral_constant<int, Is>{}), ...);
+}
+// f(std::integral_constant<int, i>) for i = 0..N-1: i is a constant expression
+// inside f, so every coefficient below is folded by the front end
+template <int N, typename F>
+__device__ __forceinline__ void static_for(F&& f) {
+  static_for_impl(f, std::make_integer_sequence<int, N>{});
+}
+
+template <typename R>
+__device__ __forceinline__ void mrt_collide_pairs(const DevParams& P, R f[19], R rho, R ux, R uy, R uz, R fx, R fy,
+                                                  R fz, R rhoN) {
+  R su, se, seps, sq, spi, sm;
+  node_rates_fast<R>(P, rhoN, su, se, seps, sq, spi, sm);
+  R pp[9], qq[9];
+  static_for<9>([&](auto kc) {
+    constexpr int k = decltype(kc)::value;
+    pp[k] = f[PREP(k)] + f[OPC(PREP(k))];
+    qq[k] = f[PREP(k)] - f[OPC(PREP(k))];
+  });
+  R m[19];
+  static_for<19>([&](auto rc) {
+    constexpr int r = decltype(rc)::value;
+    constexpr bool even = MEVEN(r);
+    R acc = R(0);
+    if constexpr (even && MROW(r, 0) != 0.0) acc = R(MROW(r, 0)) * f[0];
+    static_for<9>([&](auto kc) {
+      constexpr int k = decltype(kc)::value;
+      constexpr double c = MROW(r, PREP(k));
+      const R v = even ? pp[k] : qq[k];
+      if constexpr (c == 1.0) acc = acc + v;
+      else if constexpr (c == -1.0) acc = acc - v;
+      else if constexpr (c != 0.0) acc = acc + R(c) * v;
+    });
+    m[r] = acc;
+  });
+  R meq[19], fk[19];
+  equilf<R, false>(meq, fk, rho, ux, uy, uz, fx, fy, fz);
+  const R s[19] = {R(1), se, seps, R(1), sq, R(1), sq, R(1), sq, su, spi, su, spi, su, su, su, sm, sm, sm};
+#pragma unroll
+  for (int k = 0; k < 19; k++) m[k] = m[k] - s[k] * (m[k] - meq[k]) + (R(1) - R(0.5) * s[k]) * fk[k];
+  {
+    R e = R(0);
+    static_for<19>([&](auto rc) {
+      constexpr int r = decltype(rc)::value;
+      if constexpr (MEVEN(r) && MINV(0, r) != 0.0) e = e + R(MINV(0, r)) * m[r];
+    });
+    f[0] = e;
+  }
+  static_for<9>([&](auto kc) {
+    constexpr int i = PREP(decltype(kc)::value);
+    R e = R(0), o = R(0);
+    static_for<19>([&](auto rc) {
+      constexpr int r = decltype(rc)::value;
+      if constexpr (MINV(i, r) != 0.0) {
+        if constexpr (MEVEN(r)) e = e + R(MINV(i, r)) * m[r];
+        else o = o + R(MINV(i, r)) * m[r];
+      }
+    });
+    f[i] = e + o;
+    f[OPC(i)] = e - o;
+  });
 }
 
 __device__ __forceinline__ void unitization(double a[3]) {

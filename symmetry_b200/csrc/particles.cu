@@ -134,7 +134,12 @@ __global__ void k_walls_pinpout_plane(DevParams P, int xplane, int id, const int
 
 // ---- Lagrange_points (Source1.f90:1799-1978) ----------------------------------
 __device__ __forceinline__ int lag_idx(const DevParams& P, long long c, int n, int k) {
-  if (P.ref) return (int)c - 1;  // 1-based coordinate -> 0-based index
+  if (P.ref) {  // 1-based coordinate -> 0-based index; a point outside the
+                // arrays (the reference's domain test leaves x < 1 and z < 1
+                // open, :1832) is clamped to the edge instead of read out of bounds
+    const long long i = c - 1;
+    return (int)(i < 0 ? 0 : (i > n - 1 ? n - 1 : i));
+  }
   long long i = c - P.origin;
   const bool periodic = !(k == 0 && P.wall_x);
   if (periodic) i = ((i % n) + n) % n;
@@ -235,23 +240,27 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
   return r;
 }
 
-// Shb (immersed area) and capillary_force2 (Source1.f90:1980-2028): one block per particle
-__global__ void k_capillary(DevParams P, sym_particles* S, const double* __restrict__ Lax,
+// Shb (immersed area) and capillary_force2 (Source1.f90:1980-2028).  The
+// 16,380 Lagrange points of a particle are split over kCapBlocks blocks that
+// write fixed-order partial sums (part[(pp-1)*kCapBlocks + block][7]);
+// k_capillary_final adds them in block order (deterministic).
+constexpr int kCapBlocks = 32;
+__global__ void k_capillary(DevParams P, const sym_particles* __restrict__ S, const double* __restrict__ Lax,
                             const double* __restrict__ Lay, const double* __restrict__ Laz,
                             const double* __restrict__ La_rhoN, const double* __restrict__ La_nx,
                             const double* __restrict__ La_ny, const double* __restrict__ La_nz,
-                            const int32_t* __restrict__ La_flag, const double* __restrict__ ds, int do_shb,
-                            int do_tension) {
+                            const int32_t* __restrict__ La_flag, const double* __restrict__ ds, int do_tension,
+                            double* part) {
   __shared__ double sh[256];
-  const int par = P.par, pp = blockIdx.x + 1;
+  const int par = P.par, pp = blockIdx.y + 1;
   const double cx = PC(S->center, par, pp, 0), cy = PC(S->center, par, pp, 1), cz = PC(S->center, par, pp, 2);
   const double k = 0.134 * 1.43;
   const bool right = (P.cita == M_PI / 2.0);
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-  for (int num = threadIdx.x; num < P.la_num; num += 256) {
+  for (int num = blockIdx.x * 256 + threadIdx.x; num < P.la_num; num += 256 * kCapBlocks) {
     const long long q = (long long)num * par + (pp - 1);
     if (La_rhoN[q] > 0.0) acc[6] += ds[q];
-    if (!La_flag[q]) continue;
+    if (!do_tension || !La_flag[q]) continue;
     double nw[3] = {Lax[q] - cx, Lay[q] - cy, Laz[q] - cz};
     const double xr[3] = {nw[0], nw[1], nw[2]};
     unitization(nw);
@@ -268,12 +277,20 @@ __global__ void k_capillary(DevParams P, sym_particles* S, const double* __restr
     veccross(xr, temp, tt);
     for (int c = 0; c < 3; c++) { acc[c] += temp[c]; acc[3 + c] += tt[c]; }
   }
-  for (int c = 0; c < 7; c++) acc[c] = block_sum<256>(acc[c], sh);
-  if (threadIdx.x == 0) {
-    if (do_tension)
-      for (int c = 0; c < 3; c++) { S->tension[c * par + pp - 1] = acc[c]; S->tension_t[c * par + pp - 1] = acc[3 + c]; }
-    if (do_shb) S->shb[pp - 1] = acc[6];
+  for (int c = 0; c < 7; c++) {
+    const double v = block_sum<256>(acc[c], sh);
+    if (threadIdx.x == 0) part[((size_t)(pp - 1) * kCapBlocks + blockIdx.x) * 7 + c] = v;
   }
+}
+__global__ void k_capillary_final(DevParams P, sym_particles* S, const double* __restrict__ part, int do_shb,
+                                  int do_tension) {
+  const int par = P.par, pp = blockIdx.x + 1, c = threadIdx.x;
+  if (c >= 7) return;
+  double s = 0.0;
+  for (int b = 0; b < kCapBlocks; b++) s += part[((size_t)(pp - 1) * kCapBlocks + b) * 7 + c];
+  if (c < 3 && do_tension) S->tension[c * par + pp - 1] = s;
+  else if (c < 6 && do_tension) S->tension_t[(c - 3) * par + pp - 1] = s;
+  else if (c == 6 && do_shb) S->shb[pp - 1] = s;
 }
 
 // ---- momentum (Source1.f90:1178-1261) ------------------------------------------
@@ -533,16 +550,20 @@ int part_lagrange_points(sym_handle* h) {
   dim3 g(blocks_for(P.la_num, 128), P.par);
   k_lagrange<<<g, 128, 0, h->st>>>(P, h->dpart, h->walls, h->rhoN, h->gx, h->gy, h->gz, h->nx, h->ny, h->nz, h->lax,
                                    h->lay, h->laz, h->larhon, h->lanx, h->lany, h->lanz, h->laflag, h->lads);
-  k_capillary<<<P.par, 256, 0, h->st>>>(P, h->dpart, h->lax, h->lay, h->laz, h->larhon, h->lanx, h->lany, h->lanz,
-                                         h->laflag, h->lads, 1, 0);
+  if ((size_t)kCapBlocks * 7 * P.par > h->red_len) return set_error(h, SYM_ERR_STATE, "capillary scratch too small");
+  k_capillary<<<dim3(kCapBlocks, P.par), 256, 0, h->st>>>(P, h->dpart, h->lax, h->lay, h->laz, h->larhon, h->lanx,
+                                                           h->lany, h->lanz, h->laflag, h->lads, 0, h->red);
+  k_capillary_final<<<P.par, 32, 0, h->st>>>(P, h->dpart, h->red, 1, 0);
   return check_cuda(h, cudaGetLastError(), "Lagrange_points");
 }
 
 int part_capillary_force2(sym_handle* h) {
   const DevParams& P = h->dp;
   if (P.par == 0) return SYM_OK;
-  k_capillary<<<P.par, 256, 0, h->st>>>(P, h->dpart, h->lax, h->lay, h->laz, h->larhon, h->lanx, h->lany, h->lanz,
-                                         h->laflag, h->lads, 0, 1);
+  if ((size_t)kCapBlocks * 7 * P.par > h->red_len) return set_error(h, SYM_ERR_STATE, "capillary scratch too small");
+  k_capillary<<<dim3(kCapBlocks, P.par), 256, 0, h->st>>>(P, h->dpart, h->lax, h->lay, h->laz, h->larhon, h->lanx,
+                                                           h->lany, h->lanz, h->laflag, h->lads, 1, h->red);
+  k_capillary_final<<<P.par, 32, 0, h->st>>>(P, h->dpart, h->red, 0, 1);
   return check_cuda(h, cudaGetLastError(), "capillary_force2");
 }
 

@@ -52,6 +52,13 @@ struct sym_handle {
   cudaGraphExec_t gexec = nullptr;
   int graph_steps = 0;
   size_t bytes = 0;
+  // Every array the handle holds from creation is carved from one device
+  // allocation (the slab): one cudaMalloc and one cudaFree per handle, no
+  // per-array rounding.  A planning pass sizes it (and answers sym_footprint)
+  // without touching the device.
+  bool planning = false;
+  char* slab = nullptr;
+  size_t slab_size = 0, slab_used = 0;
   std::string err;
 };
 
@@ -60,6 +67,8 @@ namespace symb200 {
 int set_error(sym_handle* h, int code, const char* fmt, ...);
 int check_cuda(sym_handle* h, cudaError_t e, const char* what);
 void fill_devparams(const sym_params& p, DevParams& d);
+int dev_carve(sym_handle* h, void** p, size_t bytes);   // zeroed device array from the slab (or cudaMalloc)
+void dev_release(sym_handle* h, void* p);               // frees only what did not come from the slab
 
 // canonical (reference-structured) kernels, ref_kernels.cu
 int ref_calmacros(sym_handle* h);
@@ -98,4 +107,9 @@ int fast_export(sym_handle* h);   // fast -> canonical
 int fast_step(sym_handle* h, int nsteps);
 int fast_step_timed(sym_handle* h, int nsteps, double ms[4]);
 int fast_enqueue_sparse(sym_handle* h, int cur, int pc);   // particles + pin fill on h->st
+int fast_neck_planes(sym_handle* h, double* out, cudaStream_t st);   // per-z red area, nz doubles
+
+// batch engine, batch.cu
+int batch_launch(sym_batch* b, int nsteps);   // enqueue nsteps graph steps, no synchronisation
+cudaStream_t batch_stream(sym_batch* b);
 }  // namespace symb200

@@ -15,7 +15,8 @@ from typing import Dict, Optional
 
 import numpy as np
 
-from .params import (FIELD_ID, INT_FIELDS, POP_FIELDS, SymParams, SymParticles)
+from .params import (FIELD_ID, INT_FIELDS, POP_FIELDS, SYM_JOB_SLAB, SYM_JOB_THREAD, SymJobResult, SymJobSpec,
+                     SymParams, SymParticles)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libsymmetry_b200.so")
@@ -84,6 +85,19 @@ def lib() -> ctypes.CDLL:
         L.sym_batch_autotune.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
         L.sym_batch_info.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int),
                                      ctypes.POINTER(ctypes.c_int)]
+        L.sym_batch_step_kernels.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        L.sym_batch_kernels_per_step.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
+        V = ctypes.c_void_p
+        L.sym_server_create.argtypes = [ctypes.c_int, ctypes.c_size_t, ctypes.c_int, ctypes.c_int,
+                                        ctypes.POINTER(V)]
+        L.sym_server_destroy.argtypes = [V]
+        L.sym_server_last_error.restype = ctypes.c_char_p
+        L.sym_server_last_error.argtypes = [V]
+        L.sym_server_submit.argtypes = [V, ctypes.POINTER(SymJobSpec), ctypes.POINTER(ctypes.c_int64)]
+        L.sym_server_tick.argtypes = [V, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+        L.sym_server_result.argtypes = [V, ctypes.c_int64, ctypes.POINTER(SymJobResult)]
+        L.sym_server_set_xchunk.argtypes = [V, ctypes.c_int, ctypes.c_int]
+        L.sym_server_stats.argtypes = [V, ctypes.c_void_p]
         L.sym_mass_momentum_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
                                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]
         _lib = L
@@ -269,6 +283,17 @@ class Batch:
         self._ck(lib().sym_batch_autotune(self.b, trial_steps, ctypes.byref(taken)), "autotune")
         return taken.value
 
+    def step_kernels(self, n: int) -> np.ndarray:
+        """n eager steps with CUDA events: ms [total, phase, particle/wall chains, collide]."""
+        ms = np.zeros(4)
+        self._ck(lib().sym_batch_step_kernels(self.b, n, ms.ctypes.data), "batch step_kernels")
+        return ms
+
+    def kernels_per_step(self) -> int:
+        k = ctypes.c_int()
+        self._ck(lib().sym_batch_kernels_per_step(self.b, ctypes.byref(k)), "kernels_per_step")
+        return k.value
+
     def info(self):
         n, t, g = ctypes.c_int64(), ctypes.c_int(), ctypes.c_int()
         self._ck(lib().sym_batch_info(self.b, ctypes.byref(n), ctypes.byref(t), ctypes.byref(g)), "info")
@@ -278,6 +303,86 @@ class Batch:
         if self.b:
             lib().sym_batch_destroy(self.b)
             self.b = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def job_spec(w, max_steps: int, stop_radius: float = 1.0, t_arrival: float = -1.0) -> SymJobSpec:
+    """The sym_job_spec of a workload (same initial state as setup_workload)."""
+    js = SymJobSpec()
+    js.p = w.params.copy()
+    g = w.gen
+    if w.kind == "thread":
+        js.kind = SYM_JOB_THREAD
+        vals = [g["radius"], g["amp"], g["wavelength"], g.get("width", 2.0), g.get("noise", 1e-4)]
+    else:
+        js.kind = SYM_JOB_SLAB
+        vals = [g["z0"], g["z1"], g.get("width", 2.0), g.get("noise", 1e-4), 0.0]
+    for k, v in enumerate(vals):
+        js.gen[k] = float(v)
+    js.seed = int(g.get("seed", 0))
+    js.max_steps = int(max_steps)
+    js.stop_radius = float(stop_radius)
+    if w.params.par:
+        q = w.particles[0]
+        for k in range(3):
+            js.center[k] = float(q["center"][k])
+            js.up[k] = float(q.get("up", [0.0, 0.0, 0.0])[k])
+    js.t_arrival = float(t_arrival)
+    return js
+
+
+class Server:
+    """Continuous-batching job server (sym_server_*)."""
+
+    def __init__(self, device: int = 0, budget_bytes: int = 160 * 10**9, slots: int = 256, check_every: int = 10):
+        self.s = ctypes.c_void_p()
+        rc = lib().sym_server_create(device, int(budget_bytes), int(slots), int(check_every), ctypes.byref(self.s))
+        if rc:
+            raise SymError(rc, "sym_server_create")
+
+    def _ck(self, rc, what):
+        if rc:
+            raise SymError(rc, f"{what}: {lib().sym_server_last_error(self.s).decode()}")
+
+    def submit(self, spec: SymJobSpec) -> int:
+        i = ctypes.c_int64()
+        self._ck(lib().sym_server_submit(self.s, ctypes.byref(spec), ctypes.byref(i)), "submit")
+        return i.value
+
+    def tick(self, max_steps: int = 0):
+        r, p = ctypes.c_int(), ctypes.c_int()
+        self._ck(lib().sym_server_tick(self.s, int(max_steps), ctypes.byref(r), ctypes.byref(p)), "tick")
+        return r.value, p.value
+
+    def result(self, job_id: int) -> SymJobResult:
+        out = SymJobResult()
+        self._ck(lib().sym_server_result(self.s, int(job_id), ctypes.byref(out)), "result")
+        return out
+
+    def set_xchunk(self, size_class: int, x: int):
+        self._ck(lib().sym_server_set_xchunk(self.s, size_class, x), "set_xchunk")
+
+    def stats(self):
+        out = np.zeros(8)
+        self._ck(lib().sym_server_stats(self.s, out.ctypes.data), "stats")
+        keys = ["node_updates", "device_ms", "done", "failed", "running", "pending", "resident_bytes", "clock_s"]
+        return dict(zip(keys, out.tolist()))
+
+    def run_until_idle(self, max_steps: int = 0):
+        while True:
+            r, p = self.tick(max_steps)
+            if r == 0 and p == 0:
+                return
+
+    def close(self):
+        if self.s:
+            lib().sym_server_destroy(self.s)
+            self.s = ctypes.c_void_p()
 
     def __del__(self):
         try:

@@ -134,3 +134,37 @@ def config_params(nx, ny, nz, *, tau_r=1.0, tau_b=None, sigma=5e-3, beta=0.7, rh
     p.alpha = alpha_deg / 180.0 * math.pi
     p.evap_lim = 1.0e-8
     return p
+
+
+# ---- serving (sym_server_*) ------------------------------------------------------
+SYM_JOB_THREAD = 0
+SYM_JOB_SLAB = 1
+JOB_STATUS = {0: "pending", 1: "running", 2: "breakup", 3: "limit", 4: "failed"}
+
+
+class SymJobSpec(ctypes.Structure):
+    """One served job (sym_job_spec): a CONFIG domain, its initial state and stop rule."""
+    _fields_ = [
+        ("p", SymParams),
+        ("kind", ctypes.c_int32), ("max_steps", ctypes.c_int32),
+        ("gen", ctypes.c_double * 5),
+        ("seed", ctypes.c_uint64),
+        ("stop_radius", ctypes.c_double),
+        ("center", ctypes.c_double * 3), ("up", ctypes.c_double * 3),
+        ("t_arrival", ctypes.c_double),
+    ]
+
+
+class SymJobResult(ctypes.Structure):
+    _fields_ = [
+        ("status", ctypes.c_int32), ("error", ctypes.c_int32), ("steps", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("breakup_step", ctypes.c_double), ("rmin", ctypes.c_double),
+        ("t_arrival", ctypes.c_double), ("t_admit", ctypes.c_double), ("t_done", ctypes.c_double),
+        ("node_updates", ctypes.c_int64),
+    ]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        d["status"] = JOB_STATUS.get(self.status, str(self.status))
+        return d
