@@ -38,6 +38,8 @@ struct DomainDesc {
   const int32_t* pout;
   const sym_particles* Sp;
   double* ffi;
+  const float* rr_old;  // 16-bit storage: reference densities (see fused.cuh)
+  float* rr_new;
   int solid;
   int pad_;
 };
@@ -48,36 +50,27 @@ struct TileEntry {
 
 constexpr int kTPB = BZ * BY;
 
-__device__ __forceinline__ int find_domain(const long long* __restrict__ off, int n, long long b) {
-  int lo = 0, hi = n - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (off[mid] <= b) lo = mid;
-    else hi = mid - 1;
-  }
-  return lo;
-}
-
+// blk[b] = (domain, block index within the domain) of phase block b
 template <typename S>
 __global__ void __launch_bounds__(256) k_phase_batch(const DomainDesc* __restrict__ descs,
-                                                     const long long* __restrict__ blk_off, int ndom) {
+                                                     const int2* __restrict__ blk) {
   using R = typename Codec<S>::R;
-  const int d = find_domain(blk_off, ndom, blockIdx.x);
-  const DomainDesc& D = descs[d];
-  const long long L = (blockIdx.x - blk_off[d]) * 256LL + threadIdx.x;
+  const int2 e = blk[blockIdx.x];
+  const DomainDesc& D = descs[e.x];
+  const long long L = (long long)e.y * 256 + threadIdx.x;
   if (D.solid)
-    phase_node<S, true>(D.P, D.pd, (const S*)D.pin, (R*)D.phic, D.walls_all, L);
+    phase_node<S, true>(D.P, D.pd, (const S*)D.pin, (R*)D.phic, D.walls_all, L, D.rr_old, D.rr_new);
   else
-    phase_node<S, false>(D.P, D.pd, (const S*)D.pin, (R*)D.phic, D.walls_all, L);
+    phase_node<S, false>(D.P, D.pd, (const S*)D.pin, (R*)D.phic, D.walls_all, L, D.rr_old, D.rr_new);
 }
 
 template <typename S>
-__global__ void __launch_bounds__(kTPB, 2) k_collide_batch(const DomainDesc* __restrict__ descs,
+__global__ void __launch_bounds__(kTPB, collide_ctas<S>()) k_collide_batch(const DomainDesc* __restrict__ descs,
                                                            const TileEntry* __restrict__ tiles, int ntiles,
                                                            int* __restrict__ counter) {
   using R = typename Codec<S>::R;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  Smem<R>& sm = *reinterpret_cast<Smem<R>*>(smem_raw);
+  Smem<S>& sm = *reinterpret_cast<Smem<S>*>(smem_raw);
   __shared__ int s_tile;
   __shared__ __align__(16) DomainDesc s_desc;
   for (;;) {
@@ -95,10 +88,10 @@ __global__ void __launch_bounds__(kTPB, 2) k_collide_batch(const DomainDesc* __r
     const DomainDesc& D = s_desc;
     if (D.solid)
       collide_tile<S, true>(D.P, D.pd, (const S*)D.pin, (S*)D.pnext, (const R*)D.phic, D.walls, D.walls_all, D.pout,
-                            D.Sp, D.ffi, e.z0, e.y0, e.xa, e.xb, sm);
+                            D.Sp, D.ffi, D.rr_old, D.rr_new, e.z0, e.y0, e.xa, e.xb, sm);
     else
       collide_tile<S, false>(D.P, D.pd, (const S*)D.pin, (S*)D.pnext, (const R*)D.phic, D.walls, D.walls_all,
-                             D.pout, D.Sp, D.ffi, e.z0, e.y0, e.xa, e.xb, sm);
+                             D.pout, D.Sp, D.ffi, D.rr_old, D.rr_new, e.z0, e.y0, e.xa, e.xb, sm);
     __syncthreads();
   }
 }
@@ -106,7 +99,7 @@ __global__ void __launch_bounds__(kTPB, 2) k_collide_batch(const DomainDesc* __r
 template <typename S>
 int set_batch_smem(cudaStream_t, int* grid_blocks, int device) {
   using R = typename Codec<S>::R;
-  const int shm = (int)sizeof(Smem<R>);
+  const int shm = (int)sizeof(Smem<S>);
   if (cudaFuncSetAttribute(k_collide_batch<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, shm) != cudaSuccess)
     return SYM_ERR_CUDA;
   int per_sm = 0, sms = 0;
@@ -127,7 +120,7 @@ struct sym_batch {
   std::vector<int> built_cur, built_pc;   // domain parities graph 0 was built for
   int steps_since_build = 0;
   DomainDesc* d_desc[2] = {nullptr, nullptr};
-  long long* d_blk_off = nullptr;
+  int2* d_blk = nullptr;          // phase block -> (domain, block in domain)
   TileEntry* d_tiles = nullptr;
   int ntiles = 0;
   long long nblocks = 0;
@@ -170,7 +163,7 @@ void free_graphs(sym_batch* b) {
 void free_tables(sym_batch* b) {
   for (int k = 0; k < 2; k++)
     if (b->d_desc[k]) { cudaFree(b->d_desc[k]); b->d_desc[k] = nullptr; }
-  if (b->d_blk_off) { cudaFree(b->d_blk_off); b->d_blk_off = nullptr; }
+  if (b->d_blk) { cudaFree(b->d_blk); b->d_blk = nullptr; }
   if (b->d_tiles) { cudaFree(b->d_tiles); b->d_tiles = nullptr; }
 }
 
@@ -192,6 +185,8 @@ DomainDesc make_desc(sym_handle* h, int cur, int pc) {
   d.pout = h->pout;
   d.Sp = h->dpart;
   d.ffi = h->ffi;
+  d.rr_old = h->fast.rref[1 - pc];
+  d.rr_new = h->fast.rref[pc];
   d.solid = (h->dp.par > 0 || h->dp.wall_x) ? 1 : 0;
   return d;
 }
@@ -227,7 +222,7 @@ template <typename S>
 int enqueue_batch_step(sym_batch* b, int k, cudaEvent_t* ev) {
   const int n = (int)b->doms.size();
   if (ev) cudaEventRecord(ev[0], b->st);
-  k_phase_batch<S><<<(unsigned)b->nblocks, 256, 0, b->st>>>(b->d_desc[k], b->d_blk_off, n);
+  k_phase_batch<S><<<(unsigned)b->nblocks, 256, 0, b->st>>>(b->d_desc[k], b->d_blk);
   if (ev) cudaEventRecord(ev[1], b->st);
   if (!b->branch.empty()) {
     cudaEventRecord(b->ev_fork, b->st);
@@ -257,7 +252,7 @@ int enqueue_batch_step(sym_batch* b, int k, cudaEvent_t* ev) {
   if (ev) cudaEventRecord(ev[2], b->st);
   cudaMemsetAsync(b->d_counter + k, 0, sizeof(int), b->st);
   using R = typename Codec<S>::R;
-  k_collide_batch<S><<<b->grid, kTPB, sizeof(Smem<R>), b->st>>>(b->d_desc[k], b->d_tiles, b->ntiles,
+  k_collide_batch<S><<<b->grid, kTPB, sizeof(Smem<S>), b->st>>>(b->d_desc[k], b->d_tiles, b->ntiles,
                                                                  b->d_counter + k);
   if (ev) cudaEventRecord(ev[3], b->st);
   return bcuda(b, cudaGetLastError(), "batch step");
@@ -308,8 +303,11 @@ int build(sym_batch* b) {
     if (int e = bcuda(b, cudaMalloc(&b->d_desc[k], sizeof(DomainDesc) * n), "descriptors")) return e;
     cudaMemcpyAsync(b->d_desc[k], desc[k].data(), sizeof(DomainDesc) * n, cudaMemcpyHostToDevice, b->st);
   }
-  if (int e = bcuda(b, cudaMalloc(&b->d_blk_off, sizeof(long long) * (n + 1)), "offsets")) return e;
-  cudaMemcpyAsync(b->d_blk_off, off.data(), sizeof(long long) * (n + 1), cudaMemcpyHostToDevice, b->st);
+  std::vector<int2> blk((size_t)off[n]);
+  for (int i = 0; i < n; i++)
+    for (long long q = off[i]; q < off[i + 1]; q++) blk[(size_t)q] = make_int2(i, (int)(q - off[i]));
+  if (int e = bcuda(b, cudaMalloc(&b->d_blk, sizeof(int2) * std::max<size_t>(1, blk.size())), "block table")) return e;
+  cudaMemcpyAsync(b->d_blk, blk.data(), sizeof(int2) * blk.size(), cudaMemcpyHostToDevice, b->st);
   if (int e = bcuda(b, cudaMalloc(&b->d_tiles, sizeof(TileEntry) * std::max(1, b->ntiles)), "tiles")) return e;
   cudaMemcpyAsync(b->d_tiles, tiles.data(), sizeof(TileEntry) * b->ntiles, cudaMemcpyHostToDevice, b->st);
   if (int e = bcuda(b, cudaStreamSynchronize(b->st), "tables")) return e;

@@ -47,6 +47,11 @@ float* phibuf<float>(sym_handle* h, int k) { return h->fast.phif[k]; }
 template <>
 float* phibuf<__half>(sym_handle* h, int k) { return h->fast.phif[k]; }
 
+// reference densities of the 16-bit storage: decoded with rr[1 - pc], written
+// by this step's phase kernel into rr[pc] (null for the other storages)
+const float* rr_old(const sym_handle* h, int pc) { return h->fast.rref[1 - pc]; }
+float* rr_new(sym_handle* h, int pc) { return h->fast.rref[pc]; }
+
 bool has_solids(const sym_handle* h) { return h->dp.par > 0 || h->dp.wall_x; }
 
 int box_extent(const sym_handle* h, double margin) { return (int)std::ceil(2.0 * (h->dp.rad + margin)) + 2; }
@@ -69,7 +74,7 @@ int enqueue_sparse(sym_handle* h, int cur, int pc) {
     for (int pp = 1; pp <= P.par; pp++)
       k_fast_prep<S><<<blocks_for(cnt), 256, 0, h->st>>>(P, pd, np, mprep, pp, h->dpart, pin_, phic, phip,
                                                          h->walls_all, h->pout, h->rhoN, h->rhoR, h->rhoB, h->fi,
-                                                         h->gx, h->gy, h->gz, h->nx, h->ny, h->nz);
+                                                         h->gx, h->gy, h->gz, h->nx, h->ny, h->nz, rr_old(h, pc));
     int e;
     if ((e = part_lagrange_points(h))) return e;
     if ((e = part_capillary_force2(h))) return e;
@@ -83,7 +88,8 @@ int enqueue_sparse(sym_handle* h, int cur, int pc) {
     const long long cr = (long long)nr * nr * nr;
     for (int pp = 1; pp <= P.par; pp++)
       k_fast_refill_import<S><<<blocks_for(cr), 256, 0, h->st>>>(P, pd, nr, mref, pp, h->dpart, pin_, phic, h->pout,
-                                                                   h->walls_old, h->ri, h->bi, h->rhoN);
+                                                                   h->walls_old, h->ri, h->bi, h->rhoN,
+                                                                   rr_old(h, pc));
   }
   // (a2) fictitious phi on solid nodes next to fluid
   if (P.wall_x) {
@@ -116,29 +122,31 @@ int enqueue_step(sym_handle* h, int cur, int pc, cudaEvent_t* ev) {
   R* phip = phibuf<S>(h, 1 - pc);
   // (a1) calmacros
   if (ev) cudaEventRecord(ev[0], h->st);
-  if (solid) k_phase<S, true><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, pin_, phic, h->walls_all);
-  else k_phase<S, false><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, pin_, phic, h->walls_all);
+  if (solid)
+    k_phase<S, true><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, pin_, phic, h->walls_all, rr_old(h, pc), rr_new(h, pc));
+  else
+    k_phase<S, false><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, pin_, phic, h->walls_all, rr_old(h, pc),
+                                                         rr_new(h, pc));
   if (ev) cudaEventRecord(ev[1], h->st);
   if (int e = enqueue_sparse<S>(h, cur, pc)) return e;
   // (a3-a9) fused derivatives + collision + recolour + stream + bounce-back
   const int xc = h->fast.xchunk > 0 ? h->fast.xchunk : XCHUNK;
   dim3 grid((P.nz + BZ - 1) / BZ, (P.ny + BY - 1) / BY, (P.nx + xc - 1) / xc);
-  const size_t shm = sizeof(Smem<R>);
+  const size_t shm = sizeof(Smem<S>);
   if (ev) cudaEventRecord(ev[2], h->st);
   if (solid)
     k_collide<S, true><<<grid, TPB, shm, h->st>>>(P, pd, pin_, pnext, phic, h->walls, h->walls_all, h->pout,
-                                                  h->dpart, h->ffi, xc);
+                                                  h->dpart, h->ffi, rr_old(h, pc), rr_new(h, pc), xc);
   else
     k_collide<S, false><<<grid, TPB, shm, h->st>>>(P, pd, pin_, pnext, phic, h->walls, h->walls_all, h->pout,
-                                                   h->dpart, h->ffi, xc);
+                                                   h->dpart, h->ffi, rr_old(h, pc), rr_new(h, pc), xc);
   if (ev) cudaEventRecord(ev[3], h->st);
   return check_cuda(h, cudaGetLastError(), "fast step");
 }
 
 template <typename S>
 int set_smem_attr(sym_handle* h) {
-  using R = typename Codec<S>::R;
-  const int shm = (int)sizeof(Smem<R>);
+  const int shm = (int)sizeof(Smem<S>);
   cudaError_t e = cudaFuncSetAttribute(k_collide<S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, shm);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_collide<S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, shm);
@@ -206,6 +214,8 @@ int fast_alloc(sym_handle* h) {
     } else {
       if (int e = dev_carve(h, (void**)&F.phif[k], sizeof(float) * pd.size())) return e;
     }
+    if (F.storage == SYM_STORE_FP16)
+      if (int e = dev_carve(h, (void**)&F.rref[k], sizeof(float) * pd.size())) return e;
   }
   if (h->planning) return SYM_OK;
   F.bytes = h->bytes - before;
@@ -219,9 +229,11 @@ void fast_free(sym_handle* h) {
     dev_release(h, F.pop[k]);
     dev_release(h, F.phi[k]);
     dev_release(h, F.phif[k]);
+    dev_release(h, F.rref[k]);
     if (F.gexec[k]) cudaGraphExecDestroy(F.gexec[k]);
     if (F.graph[k]) cudaGraphDestroy(F.graph[k]);
-    F.pop[k] = nullptr; F.phi[k] = nullptr; F.phif[k] = nullptr; F.gexec[k] = nullptr; F.graph[k] = nullptr;
+    F.pop[k] = nullptr; F.phi[k] = nullptr; F.phif[k] = nullptr; F.rref[k] = nullptr;
+    F.gexec[k] = nullptr; F.graph[k] = nullptr;
   }
 }
 
@@ -235,15 +247,16 @@ int fast_import(sym_handle* h) {
   F.pc = 0;
   switch (F.storage) {
     case SYM_STORE_FP64:
-      k_import_pops<double><<<blocks_for(P.N), 256, 0, h->st>>>(P, h->ri, h->bi, popbuf<double>(h, 0));
+      k_import_pops<double><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, h->ri, h->bi, popbuf<double>(h, 0), nullptr);
       k_import_phi<double><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, h->rhoN, F.phi[1]);
       break;
     case SYM_STORE_FP32:
-      k_import_pops<float><<<blocks_for(P.N), 256, 0, h->st>>>(P, h->ri, h->bi, popbuf<float>(h, 0));
+      k_import_pops<float><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, h->ri, h->bi, popbuf<float>(h, 0), nullptr);
       k_import_phi<float><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, h->rhoN, F.phif[1]);
       break;
     default:
-      k_import_pops<__half><<<blocks_for(P.N), 256, 0, h->st>>>(P, h->ri, h->bi, popbuf<__half>(h, 0));
+      // after import pc = 0: the next phase decodes with rref[1]
+      k_import_pops<__half><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, h->ri, h->bi, popbuf<__half>(h, 0), F.rref[1]);
       k_import_phi<float><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, h->rhoN, F.phif[1]);
   }
   return check_cuda(h, cudaStreamSynchronize(h->st), "fast import");
@@ -257,15 +270,16 @@ int fast_export(sym_handle* h) {
   const Pad pd = make_pad(P);
   switch (F.storage) {
     case SYM_STORE_FP64:
-      k_export_pops<double><<<blocks_for(P.N), 256, 0, h->st>>>(P, popbuf<double>(h, F.cur), h->ri, h->bi);
+      k_export_pops<double><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, popbuf<double>(h, F.cur), nullptr, h->ri, h->bi);
       k_export_phi<double><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, F.phi[1 - F.pc], h->rhoN);
       break;
     case SYM_STORE_FP32:
-      k_export_pops<float><<<blocks_for(P.N), 256, 0, h->st>>>(P, popbuf<float>(h, F.cur), h->ri, h->bi);
+      k_export_pops<float><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, popbuf<float>(h, F.cur), nullptr, h->ri, h->bi);
       k_export_phi<float><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, F.phif[1 - F.pc], h->rhoN);
       break;
     default:
-      k_export_pops<__half><<<blocks_for(P.N), 256, 0, h->st>>>(P, popbuf<__half>(h, F.cur), h->ri, h->bi);
+      k_export_pops<__half><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, popbuf<__half>(h, F.cur), F.rref[1 - F.pc],
+                                                                 h->ri, h->bi);
       k_export_phi<float><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, F.phif[1 - F.pc], h->rhoN);
   }
   if (int e = check_cuda(h, cudaGetLastError(), "fast export")) return e;

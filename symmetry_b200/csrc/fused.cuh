@@ -50,17 +50,23 @@ __device__ __forceinline__ void phi_store(const DevParams& P, const Pad& pd, R* 
 // aligned 2-slot load or store per velocity (8/16-byte pairs, 4-byte for the
 // 16-bit storage), so a warp moves whole 128-byte lines per instruction.
 // FP64 / FP32: the pair is (r, b).  16-bit storage: the low half holds
-// q = f/(w rho0) - 1 in FP16 (the deviation of the total population from its
-// rest equilibrium w rho0), the high half the colour fraction c = r/f as
-// 16-bit fixed point k = 16384 + 32768 c over c in [-0.5, 1.5) (step 3.05e-5;
-// the pure phases c = 0 and c = 1 are the exact codes 16384 and 49152).
+// q = 4096 (f/(w rho_ref) - 1) in FP16 -- the deviation of the total
+// population from the rest equilibrium w rho_ref of the node it is stored at,
+// with rho_ref that node's density of the step that wrote it (so the Laplace
+// pressure jump of a drop or thread does not eat the significand, and the
+// 2^12 scale keeps deviations down to 1e-8 out of the FP16 subnormal range)
+// -- and the high half the colour fraction c = r/f as 16-bit fixed point
+// k = 16384 + 32768 c over c in [-0.5, 1.5) (step 3.05e-5; the pure phases
+// c = 0 and c = 1 are the exact codes 16384 and 49152).
 // Indices are 32-bit pair offsets (the fused path requires 38*N < 2^32).
-// load takes rho0, store takes 1/rho0 (only the 16-bit codec uses them).
+// load takes the node's rho_ref, store takes 1/rho_ref of the destination
+// node (only the 16-bit codec uses them; kRef says whether it does).
 template <typename S>
 struct Codec;
 template <>
 struct Codec<double> {
   using R = double;
+  static constexpr bool kRef = false;
   template <int I>
   __device__ __forceinline__ static void load(const double* __restrict__ p, unsigned N, unsigned L, R, R& r, R& b) {
     const double2 v = reinterpret_cast<const double2*>(p)[I * N + L];
@@ -75,6 +81,7 @@ struct Codec<double> {
 template <>
 struct Codec<float> {
   using R = float;
+  static constexpr bool kRef = false;
   template <int I>
   __device__ __forceinline__ static void load(const float* __restrict__ p, unsigned N, unsigned L, R, R& r, R& b) {
     const float2 v = reinterpret_cast<const float2*>(p)[I * N + L];
@@ -89,25 +96,30 @@ struct Codec<float> {
 template <>
 struct Codec<__half> {
   using R = float;
+  static constexpr bool kRef = true;
   template <int I>
-  __device__ __forceinline__ static void load(const __half* __restrict__ p, unsigned N, unsigned L, R rho0, R& r,
+  __device__ __forceinline__ static void load(const __half* __restrict__ p, unsigned N, unsigned L, R rref, R& r,
                                               R& b) {
     const unsigned w = reinterpret_cast<const unsigned*>(p)[I * N + L];
     const R q = __half2float(__ushort_as_half((unsigned short)(w & 0xffffu)));
-    const R c = fmaf((R)(w >> 16), 1.0f / 32768.0f, -0.5f);
-    const R wr = R(W(I)) * rho0;
-    const R f = fmaf(wr, q, wr);
+    // the colour code k sits in the low mantissa bits of 2^23 + k, so it
+    // reaches FP32 without a conversion instruction; c = k/32768 - 1/2 exactly
+    const R kf = __uint_as_float(0x4B000000u | (w >> 16));
+    const R c = fmaf(kf, 1.0f / 32768.0f, -(8388608.0f + 16384.0f) / 32768.0f);
+    const R wr = R(W(I)) * rref;
+    const R f = fmaf(wr * (1.0f / 4096.0f), q, wr);
     r = f * c;
     b = f - r;
   }
   template <int I>
-  __device__ __forceinline__ static void store(__half* p, unsigned N, unsigned L, R irho0, R r, R f) {
-    const R q = f * (R(1.0 / W(I)) * irho0) - R(1);
-    const R c = __fdividef(r, f);
-    const R kf = fminf(fmaxf(fmaf(c, 32768.0f, 16384.0f), 0.0f), 65535.0f);
+  __device__ __forceinline__ static void store(__half* p, unsigned N, unsigned L, R irref, R r, R f) {
+    const R q = f * (R(4096.0 / W(I)) * irref) - R(4096);
+    const R c = fminf(fmaxf(__fdividef(r, f), -0.5f), 1.4999694824f);   // codes 0..65535
+    // 2^23 + 16384 + 32768 c rounds to an integer whose low 16 bits are the
+    // code (nearest, ties to even): no float-to-integer conversion needed
+    const R kf = fmaf(c, 32768.0f, 8388608.0f + 16384.0f);
     const unsigned lo = __half_as_ushort(__float2half_rn(q));
-    const unsigned hi = __float2uint_rn(kf);
-    reinterpret_cast<unsigned*>(p)[I * N + L] = lo | (hi << 16);
+    reinterpret_cast<unsigned*>(p)[I * N + L] = __byte_perm(lo, __float_as_uint(kf), 0x5410);
   }
 };
 
@@ -121,35 +133,45 @@ __device__ __forceinline__ void unroll19(F&& f) {
 }
 
 // ---- k_phase: calmacros (Source1.f90:770-831) on the fused state ------------------
+// rr_old / rr_new (16-bit storage only, else null): the reference densities
+// the populations were encoded with, and this step's densities (written with
+// their periodic ghost images like phi) for the encoders of this step.
 template <typename S, bool SOLID>
 __device__ __forceinline__ void phase_node(const DevParams& P, const Pad& pd, const S* __restrict__ pops,
                                            typename Codec<S>::R* __restrict__ phi,
-                                           const int32_t* __restrict__ walls_all, long long L) {
+                                           const int32_t* __restrict__ walls_all, long long L,
+                                           const float* __restrict__ rr_old, float* __restrict__ rr_new) {
   using R = typename Codec<S>::R;
   if (L >= P.N) return;
-  const int z = (int)(L % P.nz), y = (int)((L / P.nz) % P.ny), x = (int)(L / ((long long)P.nz * P.ny));
+  // 32-bit index arithmetic (the fused path keeps 38*N < 2^32)
+  const unsigned Lu = (unsigned)L, q = Lu / (unsigned)P.nz;
+  const int z = (int)(Lu - q * (unsigned)P.nz), x = (int)(q / (unsigned)P.ny), y = (int)(q - (unsigned)x * P.ny);
   R v = R(0);
+  R rho = R(P.rho0);
   if (!(SOLID && walls_all[L] >= 1)) {
     const unsigned N = (unsigned)P.N;
-    const R rho0 = R(P.rho0);
+    const R rref = Codec<S>::kRef ? R(rr_old[pd.idx(x, y, z)]) : R(P.rho0);
     R sr = R(0), sb = R(0);
     unroll19([&](auto ic) {
       constexpr int i = decltype(ic)::value;
       R r, b;
-      Codec<S>::template load<i>(pops, N, (unsigned)L, rho0, r, b);
+      Codec<S>::template load<i>(pops, N, (unsigned)L, rref, r, b);
       sr = sr + r;
       sb = sb + b;
     });
-    v = (sr - sb) / (sr + sb);
+    rho = sr + sb;
+    v = (sr - sb) / rho;
   }
   phi_store<R>(P, pd, phi, x, y, z, v);
+  if (Codec<S>::kRef) phi_store<float>(P, pd, rr_new, x, y, z, float(rho));
 }
 
 template <typename S, bool SOLID>
 __global__ void __launch_bounds__(256) k_phase(DevParams P, Pad pd, const S* __restrict__ pops,
                                                typename Codec<S>::R* __restrict__ phi,
-                                               const int32_t* __restrict__ walls_all) {
-  phase_node<S, SOLID>(P, pd, pops, phi, walls_all, blockIdx.x * 256LL + threadIdx.x);
+                                               const int32_t* __restrict__ walls_all, const float* __restrict__ rr_old,
+                                               float* __restrict__ rr_new) {
+  phase_node<S, SOLID>(P, pd, pops, phi, walls_all, blockIdx.x * 256LL + threadIdx.x, rr_old, rr_new);
 }
 
 // ---- wetting rotation of a node normal (derivatives :535-587) ---------------------
@@ -169,10 +191,12 @@ __device__ __forceinline__ void wet_rotate(const DevParams& P, const sym_particl
 // phi ring of 5 planes and normal ring of 4 planes: with normals computed one
 // plane ahead and phi loaded three planes ahead, one barrier per plane keeps
 // every slot a warp may still read distinct from the slots being written.
-template <typename R>
+template <typename S>
 struct Smem {
+  using R = typename Codec<S>::R;
   R phi[5][BY + 4][BZ + 4];
   R n[4][4][BY + 2][BZ + 2];   // [plane][nx,ny,nz,|grad|][y][z]
+  float irr[Codec<S>::kRef ? 5 : 1][BY + 4][BZ + 4];   // 1/rho_ref of this step (16-bit storage)
 };
 
 // One tile: the 32(z) x 8(y) footprint at (z0, y0), planes xa..xb-1.  Called
@@ -185,23 +209,32 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
                                              const int32_t* __restrict__ walls_all,
                                              const int32_t* __restrict__ pout,
                                              const sym_particles* __restrict__ Sp, double* __restrict__ ffi,
-                                             int z0, int y0, int xa, int xb, Smem<typename Codec<S>::R>& sm) {
+                                             const float* __restrict__ rr_old, const float* __restrict__ rr_new,
+                                             int z0, int y0, int xa, int xb, Smem<S>& sm) {
   using R = typename Codec<S>::R;
+  constexpr bool REF = Codec<S>::kRef;
   const int tz = threadIdx.x % BZ, ty = threadIdx.x / BZ;
   const unsigned N = (unsigned)P.N;
-  const R rho0 = R(P.rho0), irho0 = R(1.0 / P.rho0);
+  const R irho0 = R(1.0 / P.rho0);
   const R evap = R(P.evap);
   const int sy = P.nz, sx = P.nz * P.ny;   // element strides of y and x
 
   // load phi plane xp (padded coordinates stay inside the ghost layers)
   auto load_phi = [&](int xp) {
-    R(*dst)[BZ + 4] = sm.phi[((xp % 5) + 5) % 5];
+    const int sl = ((xp % 5) + 5) % 5;
+    R(*dst)[BZ + 4] = sm.phi[sl];
     for (int t = threadIdx.x; t < (BY + 4) * (BZ + 4); t += TPB) {
       const int py = t / (BZ + 4), pz = t % (BZ + 4);
       const int y = y0 - 2 + py, z = z0 - 2 + pz;
       R v = R(0);
-      if (y <= P.ny + 1 && z <= P.nz + 1) v = phi[pd.idx(xp, y, z)];
+      float ir = 1.0f;
+      if (y <= P.ny + 1 && z <= P.nz + 1) {
+        const long long q = pd.idx(xp, y, z);
+        v = phi[q];
+        if (REF) ir = 1.0f / rr_new[q];
+      }
       dst[py][pz] = v;
+      if (REF) sm.irr[sl][py][pz] = ir;
     }
   };
   // unit normal (rotated at wetting nodes) and |grad phi| of plane xp, halo 1
@@ -270,10 +303,11 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
     // calmacros on the own populations
     R f[19];
     R sr = R(0), sb = R(0);
+    const R rref = REF ? R(rr_old[pd.idx(x, y, z)]) : R(P.rho0);
     unroll19([&](auto ic) {
       constexpr int i = decltype(ic)::value;
       R r, b;
-      Codec<S>::template load<i>(pin_, N, L, rho0, r, b);
+      Codec<S>::template load<i>(pin_, N, L, rref, r, b);
       f[i] = r + b;
       sr = sr + r;
       sb = sb + b;
@@ -365,30 +399,38 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
           }
           const R rr = r + R(6.0 * W(j)) * sr * star;
           const R bb = (f[i] - r) + R(6.0 * W(j)) * sb * star;
-          Codec<S>::template store<j>(pout_, N, L, irho0, rr, rr + bb);
+          const R irr = REF ? R(sm.irr[x % 5][ty + 2][tz + 2]) : irho0;
+          Codec<S>::template store<j>(pout_, N, L, irr, rr, rr + bb);
           return;
         }
       }
-      Codec<S>::template store<i>(pout_, N, T, irho0, r, f[i]);
+      const R irr = REF ? R(sm.irr[(x + CX(i) + 5) % 5][ty + 2 + CY(i)][tz + 2 + CZ(i)]) : irho0;
+      Codec<S>::template store<i>(pout_, N, T, irr, r, f[i]);
     });
   }
 }
 
+// Resident CTAs per SM the collide kernels are compiled for: the FP32-math
+// codecs fit 80 registers without spilling (3 CTAs of 256 threads), FP64
+// needs the 128 of 2 CTAs.
+template <typename S>
+constexpr int collide_ctas() { return sizeof(typename Codec<S>::R) == 4 ? 3 : 2; }
+
 template <typename S, bool SOLID>
-__global__ void __launch_bounds__(TPB, 2) k_collide(DevParams P, Pad pd, const S* __restrict__ pin_,
+__global__ void __launch_bounds__(TPB, collide_ctas<S>()) k_collide(DevParams P, Pad pd, const S* __restrict__ pin_,
                                                    S* __restrict__ pout_,
                                                    const typename Codec<S>::R* __restrict__ phi,
                                                    const int32_t* __restrict__ walls,
                                                    const int32_t* __restrict__ walls_all,
                                                    const int32_t* __restrict__ pout,
                                                    const sym_particles* __restrict__ Sp, double* __restrict__ ffi,
+                                                   const float* __restrict__ rr_old, const float* __restrict__ rr_new,
                                                    int xchunk) {
-  using R = typename Codec<S>::R;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  Smem<R>& sm = *reinterpret_cast<Smem<R>*>(smem_raw);
+  Smem<S>& sm = *reinterpret_cast<Smem<S>*>(smem_raw);
   const int xa = blockIdx.z * xchunk;
-  collide_tile<S, SOLID>(P, pd, pin_, pout_, phi, walls, walls_all, pout, Sp, ffi, blockIdx.x * BZ, blockIdx.y * BY,
-                         xa, min(xa + xchunk, P.nx), sm);
+  collide_tile<S, SOLID>(P, pd, pin_, pout_, phi, walls, walls_all, pout, Sp, ffi, rr_old, rr_new, blockIdx.x * BZ,
+                         blockIdx.y * BY, xa, min(xa + xchunk, P.nx), sm);
 }
 
 // ---- pin fill on the fused state (derivatives :467-492) ----------------------------
@@ -461,13 +503,13 @@ __global__ void k_fast_prep(DevParams P, Pad pd, int n, double margin, int pp, c
                             const typename Codec<S>::R* __restrict__ phi_prev,
                             const int32_t* __restrict__ walls_all, const int32_t* __restrict__ pout,
                             double* rhoN, double* rhoR, double* rhoB, double* fi, double* gx, double* gy,
-                            double* gz, double* nxv, double* nyv, double* nzv) {
+                            double* gz, double* nxv, double* nyv, double* nzv, const float* __restrict__ rr_old) {
   using R = typename Codec<S>::R;
   int x, y, z;
   if (!fbox_node(P, n, margin, Sp->center, pp, blockIdx.x * (long long)blockDim.x + threadIdx.x, x, y, z)) return;
   const long long L = lin(P, x, y, z);
   const unsigned N = (unsigned)P.N;
-  const R rho0 = R(P.rho0);
+  const R rref = Codec<S>::kRef ? R(rr_old[pd.idx(x, y, z)]) : R(P.rho0);
   if (walls_all[L] > 0) {
     rhoN[L] = 0.0;
     gx[L] = 0.0; gy[L] = 0.0; gz[L] = 0.0; nxv[L] = 0.0; nyv[L] = 0.0; nzv[L] = 0.0;
@@ -477,7 +519,7 @@ __global__ void k_fast_prep(DevParams P, Pad pd, int n, double margin, int pp, c
   unroll19([&](auto ic) {
     constexpr int i = decltype(ic)::value;
     R r, b;
-    Codec<S>::template load<i>(pops, N, (unsigned)L, rho0, r, b);
+    Codec<S>::template load<i>(pops, N, (unsigned)L, rref, r, b);
     fi[(size_t)i * N + L] = (double)(r + b);
     sr = sr + r;
     sb = sb + b;
@@ -512,7 +554,8 @@ __global__ void k_fast_refill_import(DevParams P, Pad pd, int n, double margin, 
                                      const sym_particles* __restrict__ Sp, S* pops,
                                      typename Codec<S>::R* phi_cur, const int32_t* __restrict__ pout,
                                      const int32_t* __restrict__ walls_old, const double* __restrict__ ri,
-                                     const double* __restrict__ bi, const double* __restrict__ rhoN) {
+                                     const double* __restrict__ bi, const double* __restrict__ rhoN,
+                                     const float* __restrict__ rr_old) {
   using R = typename Codec<S>::R;
   int x, y, z;
   if (!fbox_node(P, n, margin, Sp->center_old, pp, blockIdx.x * (long long)blockDim.x + threadIdx.x, x, y, z))
@@ -520,40 +563,59 @@ __global__ void k_fast_refill_import(DevParams P, Pad pd, int n, double margin, 
   const long long L = lin(P, x, y, z);
   const unsigned N = (unsigned)P.N;
   if (pout[L] != pp || walls_old[L] < 1) return;
-  const R irho0 = R(1.0 / P.rho0);
+  // the collide of this step decodes these populations with rr_old
+  const R irr = Codec<S>::kRef ? R(1) / R(rr_old[pd.idx(x, y, z)]) : R(1.0 / P.rho0);
   unroll19([&](auto ic) {
     constexpr int i = decltype(ic)::value;
     const R r = R(ri[(size_t)i * N + L]), b = R(bi[(size_t)i * N + L]);
-    Codec<S>::template store<i>(pops, N, (unsigned)L, irho0, r, r + b);
+    Codec<S>::template store<i>(pops, N, (unsigned)L, irr, r, r + b);
   });
   phi_store<R>(P, pd, phi_cur, x, y, z, R(rhoN[L]));
 }
 
 // whole-domain conversions between the canonical arrays and the fused state
+// rr (16-bit storage, else null): receives each node's density, the
+// reference its populations are encoded with (a solid or empty node keeps rho0)
 template <typename S>
-__global__ void k_import_pops(DevParams P, const double* __restrict__ ri, const double* __restrict__ bi, S* pops) {
+__global__ void k_import_pops(DevParams P, Pad pd, const double* __restrict__ ri, const double* __restrict__ bi,
+                              S* pops, float* rr) {
   using R = typename Codec<S>::R;
   const long long L = blockIdx.x * 256LL + threadIdx.x;
   if (L >= P.N) return;
   const unsigned N = (unsigned)P.N;
-  const R irho0 = R(1.0 / P.rho0);
+  R irr = R(1.0 / P.rho0);
+  if (Codec<S>::kRef) {
+    double rho = 0.0;
+    for (int i = 0; i < 19; i++) rho += ri[(size_t)i * N + L] + bi[(size_t)i * N + L];
+    const float ref = rho > 0.0 ? float(rho) : float(P.rho0);
+    const unsigned Lu = (unsigned)L, q = Lu / (unsigned)P.nz;
+    const int z = (int)(Lu - q * (unsigned)P.nz), x = (int)(q / (unsigned)P.ny), y = (int)(q - (unsigned)x * P.ny);
+    phi_store<float>(P, pd, rr, x, y, z, ref);
+    irr = R(1) / R(ref);
+  }
   unroll19([&](auto ic) {
     constexpr int i = decltype(ic)::value;
     const R r = R(ri[(size_t)i * N + L]), b = R(bi[(size_t)i * N + L]);
-    Codec<S>::template store<i>(pops, N, (unsigned)L, irho0, r, r + b);
+    Codec<S>::template store<i>(pops, N, (unsigned)L, irr, r, r + b);
   });
 }
 template <typename S>
-__global__ void k_export_pops(DevParams P, const S* __restrict__ pops, double* ri, double* bi) {
+__global__ void k_export_pops(DevParams P, Pad pd, const S* __restrict__ pops, const float* __restrict__ rr, double* ri,
+                              double* bi) {
   using R = typename Codec<S>::R;
   const long long L = blockIdx.x * 256LL + threadIdx.x;
   if (L >= P.N) return;
   const unsigned N = (unsigned)P.N;
-  const R rho0 = R(P.rho0);
+  R rref = R(P.rho0);
+  if (Codec<S>::kRef) {
+    const unsigned Lu = (unsigned)L, q = Lu / (unsigned)P.nz;
+    const int z = (int)(Lu - q * (unsigned)P.nz), x = (int)(q / (unsigned)P.ny), y = (int)(q - (unsigned)x * P.ny);
+    rref = R(rr[pd.idx(x, y, z)]);
+  }
   unroll19([&](auto ic) {
     constexpr int i = decltype(ic)::value;
     R r, b;
-    Codec<S>::template load<i>(pops, N, (unsigned)L, rho0, r, b);
+    Codec<S>::template load<i>(pops, N, (unsigned)L, rref, r, b);
     ri[(size_t)i * N + L] = (double)r;
     bi[(size_t)i * N + L] = (double)b;
   });

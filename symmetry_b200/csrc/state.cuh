@@ -18,6 +18,7 @@ struct FastState {
   int xchunk = 0;          // x planes per tile of the fused collide kernel (0 = default)
   double* phi[2] = {nullptr, nullptr};  // FP64 halo-padded phase field (pin-filled)
   float* phif[2] = {nullptr, nullptr};  // FP32 halo-padded phase field for FP32/FP16 storage
+  float* rref[2] = {nullptr, nullptr};  // 16-bit storage: halo-padded reference densities (same parity as phi)
   bool valid = false;      // fast state holds the authoritative populations
   size_t bytes = 0;
   cudaGraph_t graph[2] = {nullptr, nullptr};       // one captured step per buffer parity
