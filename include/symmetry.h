@@ -326,8 +326,10 @@ int sym_mass_momentum(sym_handle* h, double out[5]);
  *   msg        optional buffer for an error message
  * The call is asynchronous on `stream`.  The first call on each device looks
  * up the scratch address (cudaGetSymbolAddress) and should come before any
- * stream capture.  Calls share the scratch: calls that overlap on the GPU
- * race, so serialise them (one stream, or events). */
+ * stream capture; the address is kept for the life of the process, so a
+ * process that resets a device (cudaDeviceReset) must not call this entry
+ * point on that device afterwards.  Calls share the scratch: calls that
+ * overlap on the GPU race, so serialise them (one stream, or events). */
 int sym_mass_momentum_noalloc(const double* ri, const double* bi, const int32_t* walls_all, int64_t n_nodes,
                               double* out, void* stream, char* msg, size_t msg_len);
 

@@ -188,15 +188,21 @@ __device__ __forceinline__ void wet_rotate(const DevParams& P, const sym_particl
 }
 
 // ---- k_collide ------------------------------------------------------------------
-// phi ring of 5 planes and normal ring of 4 planes: with normals computed one
-// plane ahead and phi loaded three planes ahead, one barrier per plane keeps
-// every slot a warp may still read distinct from the slots being written.
+// phi ring of 5 planes, normal ring of 4 planes, 1/rho_ref ring of 6 planes:
+// normals are computed one plane ahead and phi / 1/rho_ref loaded three planes
+// ahead, before the plane's single barrier.  A warp that has finished plane x
+// runs those writes for plane x+1 while slower warps still read plane x's
+// slots: phi at x, normals at x-1..x+1 and 1/rho_ref at x-1..x+1 (the push
+// targets).  The rings are sized so that the slots written for plane x+1
+// (phi x+4 -> slot (x-1)%5, normals x+2 -> (x-2)%4, 1/rho_ref x+4 -> (x-2)%6)
+// are never among them.
+constexpr int kIrrRing = 6;
 template <typename S>
 struct Smem {
   using R = typename Codec<S>::R;
   R phi[5][BY + 4][BZ + 4];
   R n[4][4][BY + 2][BZ + 2];   // [plane][nx,ny,nz,|grad|][y][z]
-  float irr[Codec<S>::kRef ? 5 : 1][BY + 4][BZ + 4];   // 1/rho_ref of this step (16-bit storage)
+  float irr[Codec<S>::kRef ? kIrrRing : 1][BY + 4][BZ + 4];   // 1/rho_ref of this step (16-bit storage)
 };
 
 // One tile: the 32(z) x 8(y) footprint at (z0, y0), planes xa..xb-1.  Called
@@ -234,7 +240,7 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
         if (REF) ir = 1.0f / rr_new[q];
       }
       dst[py][pz] = v;
-      if (REF) sm.irr[sl][py][pz] = ir;
+      if (REF) sm.irr[((xp % kIrrRing) + kIrrRing) % kIrrRing][py][pz] = ir;
     }
   };
   // unit normal (rotated at wetting nodes) and |grad phi| of plane xp, halo 1
@@ -399,12 +405,12 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
           }
           const R rr = r + R(6.0 * W(j)) * sr * star;
           const R bb = (f[i] - r) + R(6.0 * W(j)) * sb * star;
-          const R irr = REF ? R(sm.irr[x % 5][ty + 2][tz + 2]) : irho0;
+          const R irr = REF ? R(sm.irr[x % kIrrRing][ty + 2][tz + 2]) : irho0;
           Codec<S>::template store<j>(pout_, N, L, irr, rr, rr + bb);
           return;
         }
       }
-      const R irr = REF ? R(sm.irr[(x + CX(i) + 5) % 5][ty + 2 + CY(i)][tz + 2 + CZ(i)]) : irho0;
+      const R irr = REF ? R(sm.irr[(x + CX(i) + kIrrRing) % kIrrRing][ty + 2 + CY(i)][tz + 2 + CZ(i)]) : irho0;
       Codec<S>::template store<i>(pout_, N, T, irr, r, f[i]);
     });
   }

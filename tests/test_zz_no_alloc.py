@@ -49,9 +49,9 @@ def test_noalloc_sums_match_handle_entry_point_twice():
             L.step(25)   # different data for the second call
         want = L.mass_momentum()
         got = _noalloc(torch, L, out)
-        # the tests' FP64 tolerance, 1e-12 of the domain's mass (momentum sums
-        # of a symmetric flow are rounding noise, so they share the mass scale)
-        assert np.all(np.abs(got - want) <= 1e-12 * (abs(want[0]) + abs(want[1]))), (call, got, want)
+        # the same populations in the same node order, the same per-node
+        # arithmetic and the same fixed reduction tree: identical bits
+        assert np.array_equal(got, want), (call, got, want)
 
 
 def test_noalloc_refuses_oversized_domain():
