@@ -1,8 +1,9 @@
 // batch.cu -- many independent CONFIG domains stepped together.
 //
 // One step of a batch is one CUDA graph:
-//   k_phase_batch     calmacros of every domain in one launch (blocks map to
-//                     domains through a prefix sum of per-domain block counts);
+//   k_finalize_batch  calmacros of every domain in one launch, from the colour
+//                     densities the previous collide accumulated (blocks map
+//                     to domains through a prefix sum of per-domain block counts);
 //   per-domain sparse particle coupling and pin fill (only domains with
 //                     solids; these are the small kernels of fast.cu), each
 //                     domain's chain on its own graph branch so the chains
@@ -40,6 +41,8 @@ struct DomainDesc {
   double* ffi;
   const float* rr_old;  // 16-bit storage: reference densities (see fused.cuh)
   float* rr_new;
+  void* acc;            // accumulated colour densities of the next step (see fused.cuh)
+  int* status;
   int solid;
   int pad_;
 };
@@ -52,16 +55,17 @@ constexpr int kTPB = BZ * BY;
 
 // blk[b] = (domain, block index within the domain) of phase block b
 template <typename S>
-__global__ void __launch_bounds__(256) k_phase_batch(const DomainDesc* __restrict__ descs,
-                                                     const int2* __restrict__ blk) {
+__global__ void __launch_bounds__(256) k_finalize_batch(const DomainDesc* __restrict__ descs,
+                                                        const int2* __restrict__ blk) {
   using R = typename Codec<S>::R;
+  using AT = typename Acc<R>::T;
   const int2 e = blk[blockIdx.x];
   const DomainDesc& D = descs[e.x];
   const long long L = (long long)e.y * 256 + threadIdx.x;
   if (D.solid)
-    phase_node<S, true>(D.P, D.pd, (const S*)D.pin, (R*)D.phic, D.walls_all, L, D.rr_old, D.rr_new);
+    finalize_node<S, true>(D.P, D.pd, (AT*)D.acc, (R*)D.phic, D.walls_all, D.rr_new, D.status, L);
   else
-    phase_node<S, false>(D.P, D.pd, (const S*)D.pin, (R*)D.phic, D.walls_all, L, D.rr_old, D.rr_new);
+    finalize_node<S, false>(D.P, D.pd, (AT*)D.acc, (R*)D.phic, D.walls_all, D.rr_new, D.status, L);
 }
 
 template <typename S>
@@ -86,12 +90,14 @@ __global__ void __launch_bounds__(kTPB, collide_ctas<S>()) k_collide_batch(const
     }
     __syncthreads();
     const DomainDesc& D = s_desc;
+    using AT = typename Acc<R>::T;
     if (D.solid)
       collide_tile<S, true>(D.P, D.pd, (const S*)D.pin, (S*)D.pnext, (const R*)D.phic, D.walls, D.walls_all, D.pout,
-                            D.Sp, D.ffi, D.rr_old, D.rr_new, e.z0, e.y0, e.xa, e.xb, sm);
+                            D.Sp, D.ffi, D.rr_old, D.rr_new, (AT*)D.acc, D.status, e.z0, e.y0, e.xa, e.xb, sm);
     else
       collide_tile<S, false>(D.P, D.pd, (const S*)D.pin, (S*)D.pnext, (const R*)D.phic, D.walls, D.walls_all,
-                             D.pout, D.Sp, D.ffi, D.rr_old, D.rr_new, e.z0, e.y0, e.xa, e.xb, sm);
+                             D.pout, D.Sp, D.ffi, D.rr_old, D.rr_new, (AT*)D.acc, D.status, e.z0, e.y0, e.xa, e.xb,
+                             sm);
     __syncthreads();
   }
 }
@@ -187,6 +193,8 @@ DomainDesc make_desc(sym_handle* h, int cur, int pc) {
   d.ffi = h->ffi;
   d.rr_old = h->fast.rref[1 - pc];
   d.rr_new = h->fast.rref[pc];
+  d.acc = h->fast.acc;
+  d.status = h->fast.status;
   d.solid = (h->dp.par > 0 || h->dp.wall_x) ? 1 : 0;
   return d;
 }
@@ -222,7 +230,7 @@ template <typename S>
 int enqueue_batch_step(sym_batch* b, int k, cudaEvent_t* ev) {
   const int n = (int)b->doms.size();
   if (ev) cudaEventRecord(ev[0], b->st);
-  k_phase_batch<S><<<(unsigned)b->nblocks, 256, 0, b->st>>>(b->d_desc[k], b->d_blk);
+  k_finalize_batch<S><<<(unsigned)b->nblocks, 256, 0, b->st>>>(b->d_desc[k], b->d_blk);
   if (ev) cudaEventRecord(ev[1], b->st);
   if (!b->branch.empty()) {
     cudaEventRecord(b->ev_fork, b->st);

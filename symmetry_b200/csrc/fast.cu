@@ -1,10 +1,11 @@
 // fast.cu -- fused fast path of the per-timestep lattice update (CONFIG mode).
 //
 // Per step (same order as the reference loop body, Source1.f90:216-251):
-//   k_phase      calmacros (a1): read the 38 own post-stream populations
-//                (aligned, coalesced), write phi into a halo-padded array
-//                (every node also writes its periodic images in the 2-deep
-//                ghost layers, so stencil tiles never wrap).
+//   k_finalize   calmacros (a1): phi = (rhoR - rhoB) / rho from the two
+//                colour densities per node that the previous step's collide
+//                kernel accumulated, written into a halo-padded array (every
+//                node also writes its periodic images in the 2-deep ghost
+//                layers, so stencil tiles never wrap).
 //   particles    sparse: Lagrange points, capillary force, momentum exchange,
 //                repulsion, Newton-Euler, set_walls, refill -- on the
 //                particle's bounding box only.
@@ -17,7 +18,10 @@
 //                pushes the recoloured post-collision populations to their
 //                neighbours (push streaming), reflecting links that enter a
 //                solid node back into the node itself (halfway bounce-back
-//                with the wall velocity term of curve).
+//                with the wall velocity term of curve).  It also adds each
+//                pushed value into its destination's colour-density
+//                accumulators (combined inside the CTA, fixed-point atomics
+//                across tiles), which the next step's k_finalize reads.
 // Populations are stored post-stream as [colour-slot][velocity][node].
 #include <cuda_fp16.h>
 #include <cmath>
@@ -54,9 +58,14 @@ float* rr_new(sym_handle* h, int pc) { return h->fast.rref[pc]; }
 
 bool has_solids(const sym_handle* h) { return h->dp.par > 0 || h->dp.wall_x; }
 
+template <typename S>
+typename Acc<typename Codec<S>::R>::T* accbuf(sym_handle* h) {
+  return reinterpret_cast<typename Acc<typename Codec<S>::R>::T*>(h->fast.acc);
+}
+
 int box_extent(const sym_handle* h, double margin) { return (int)std::ceil(2.0 * (h->dp.rad + margin)) + 2; }
 
-// sparse per-step work between k_phase and k_collide: particle coupling on
+// sparse per-step work between k_finalize and k_collide: particle coupling on
 // the particle boxes and the fictitious phi on solid nodes next to fluid
 template <typename S>
 int enqueue_sparse(sym_handle* h, int cur, int pc) {
@@ -108,7 +117,7 @@ int enqueue_sparse(sym_handle* h, int cur, int pc) {
   return check_cuda(h, cudaGetLastError(), "fast sparse step");
 }
 
-// ev (optional): 4 events recorded before k_phase, after k_phase, before
+// ev (optional): 4 events recorded before k_finalize, after it, before
 // k_collide and after k_collide, for per-kernel timing on the library stream
 template <typename S>
 int enqueue_step(sym_handle* h, int cur, int pc, cudaEvent_t* ev) {
@@ -120,13 +129,14 @@ int enqueue_step(sym_handle* h, int cur, int pc, cudaEvent_t* ev) {
   S* pnext = popbuf<S>(h, 1 - cur);
   R* phic = phibuf<S>(h, pc);
   R* phip = phibuf<S>(h, 1 - pc);
-  // (a1) calmacros
+  // (a1) calmacros from the colour densities the previous collide accumulated
   if (ev) cudaEventRecord(ev[0], h->st);
   if (solid)
-    k_phase<S, true><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, pin_, phic, h->walls_all, rr_old(h, pc), rr_new(h, pc));
+    k_finalize<S, true><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, accbuf<S>(h), phic, h->walls_all, rr_new(h, pc),
+                                                            h->fast.status);
   else
-    k_phase<S, false><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, pin_, phic, h->walls_all, rr_old(h, pc),
-                                                         rr_new(h, pc));
+    k_finalize<S, false><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, accbuf<S>(h), phic, h->walls_all, rr_new(h, pc),
+                                                             h->fast.status);
   if (ev) cudaEventRecord(ev[1], h->st);
   if (int e = enqueue_sparse<S>(h, cur, pc)) return e;
   // (a3-a9) fused derivatives + collision + recolour + stream + bounce-back
@@ -136,10 +146,12 @@ int enqueue_step(sym_handle* h, int cur, int pc, cudaEvent_t* ev) {
   if (ev) cudaEventRecord(ev[2], h->st);
   if (solid)
     k_collide<S, true><<<grid, TPB, shm, h->st>>>(P, pd, pin_, pnext, phic, h->walls, h->walls_all, h->pout,
-                                                  h->dpart, h->ffi, rr_old(h, pc), rr_new(h, pc), xc);
+                                                  h->dpart, h->ffi, rr_old(h, pc), rr_new(h, pc), accbuf<S>(h),
+                                                  h->fast.status, xc);
   else
     k_collide<S, false><<<grid, TPB, shm, h->st>>>(P, pd, pin_, pnext, phic, h->walls, h->walls_all, h->pout,
-                                                   h->dpart, h->ffi, rr_old(h, pc), rr_new(h, pc), xc);
+                                                   h->dpart, h->ffi, rr_old(h, pc), rr_new(h, pc), accbuf<S>(h),
+                                                   h->fast.status, xc);
   if (ev) cudaEventRecord(ev[3], h->st);
   return check_cuda(h, cudaGetLastError(), "fast step");
 }
@@ -217,6 +229,8 @@ int fast_alloc(sym_handle* h) {
     if (F.storage == SYM_STORE_FP16)
       if (int e = dev_carve(h, (void**)&F.rref[k], sizeof(float) * pd.size())) return e;
   }
+  if (int e = dev_carve(h, &F.acc, 2 * h->N * (F.storage == SYM_STORE_FP64 ? 8 : 4))) return e;
+  if (int e = dev_carve(h, (void**)&F.status, sizeof(int))) return e;
   if (h->planning) return SYM_OK;
   F.bytes = h->bytes - before;
   return F.storage == SYM_STORE_FP64 ? set_smem_attr<double>(h)
@@ -230,6 +244,12 @@ void fast_free(sym_handle* h) {
     dev_release(h, F.phi[k]);
     dev_release(h, F.phif[k]);
     dev_release(h, F.rref[k]);
+    if (k == 0) {
+      dev_release(h, F.acc);
+      dev_release(h, (void*)F.status);
+      F.acc = nullptr;
+      F.status = nullptr;
+    }
     if (F.gexec[k]) cudaGraphExecDestroy(F.gexec[k]);
     if (F.graph[k]) cudaGraphDestroy(F.graph[k]);
     F.pop[k] = nullptr; F.phi[k] = nullptr; F.phif[k] = nullptr; F.rref[k] = nullptr;
@@ -245,18 +265,22 @@ int fast_import(sym_handle* h) {
   const Pad pd = make_pad(P);
   F.cur = 0;
   F.pc = 0;
+  cudaMemsetAsync(F.status, 0, sizeof(int), h->st);
   switch (F.storage) {
     case SYM_STORE_FP64:
-      k_import_pops<double><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, h->ri, h->bi, popbuf<double>(h, 0), nullptr);
+      k_import_pops<double><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, h->ri, h->bi, popbuf<double>(h, 0), nullptr,
+                                                                accbuf<double>(h), F.status);
       k_import_phi<double><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, h->rhoN, F.phi[1]);
       break;
     case SYM_STORE_FP32:
-      k_import_pops<float><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, h->ri, h->bi, popbuf<float>(h, 0), nullptr);
+      k_import_pops<float><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, h->ri, h->bi, popbuf<float>(h, 0), nullptr,
+                                                               accbuf<float>(h), F.status);
       k_import_phi<float><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, h->rhoN, F.phif[1]);
       break;
     default:
       // after import pc = 0: the next phase decodes with rref[1]
-      k_import_pops<__half><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, h->ri, h->bi, popbuf<__half>(h, 0), F.rref[1]);
+      k_import_pops<__half><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, h->ri, h->bi, popbuf<__half>(h, 0), F.rref[1],
+                                                                accbuf<__half>(h), F.status);
       k_import_phi<float><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, h->rhoN, F.phif[1]);
   }
   return check_cuda(h, cudaStreamSynchronize(h->st), "fast import");
@@ -312,7 +336,7 @@ int fast_step(sym_handle* h, int nsteps) {
 }
 
 // nsteps eager (not graph) steps with CUDA events around the kernel classes.
-// ms[0] = whole region, ms[1] = sum of k_phase, ms[2] = sum of the sparse
+// ms[0] = whole region, ms[1] = sum of k_finalize, ms[2] = sum of the sparse
 // particle/pin-fill work, ms[3] = sum of k_collide.
 int fast_enqueue_sparse(sym_handle* h, int cur, int pc) { return enqueue_sparse_any(h, cur, pc); }
 

@@ -123,6 +123,45 @@ struct Codec<__half> {
   }
 };
 
+// ---- next-step colour densities accumulated by the collide kernel ----------------
+// The collide kernel of a step pushes every post-collision population to the
+// node that holds it after streaming; it also adds the pushed values per
+// destination node into two fixed-point accumulators (red, blue), so the next
+// step's phase field (calmacros) reads 2 numbers per node instead of all 38
+// populations.  Integer addition is associative, so the totals do not depend
+// on the order in which the tiles' atomic adds land: the accumulated densities
+// are deterministic.  FP64 storage: 64-bit integers in units of 2^-52
+// (|rho| < 1024); FP32 arithmetic: 32-bit integers in units of 2^-26
+// (|rho| < 31).  A value outside that range or not finite sets the domain's
+// status word, and the next phase field is written as NaN (the NaN test of the
+// stop rule then retires the run).
+template <typename R>
+struct Acc;
+template <>
+struct Acc<double> {
+  using T = unsigned long long;
+  __device__ __forceinline__ static T fix(double v) { return (T)__double2ll_rn(v * 0x1p52); }
+  __device__ __forceinline__ static double val(T a) { return (double)(long long)a * 0x1p-52; }
+  __device__ __forceinline__ static bool ok(double v) { return fabs(v) < 1024.0; }
+};
+template <>
+struct Acc<float> {
+  using T = unsigned int;
+  __device__ __forceinline__ static T fix(float v) { return (T)__float2int_rn(v * 0x1p26f); }
+  __device__ __forceinline__ static float val(T a) { return (float)(int)a * 0x1p-26f; }
+  __device__ __forceinline__ static bool ok(float v) { return fabsf(v) < 31.0f; }
+};
+// add v to accumulator p (a reduction: nothing is returned); out-of-range
+// values set *status and add nothing
+template <typename R>
+__device__ __forceinline__ void acc_add(typename Acc<R>::T* p, R v, int* status) {
+  if (Acc<R>::ok(v)) {
+    atomicAdd(p, Acc<R>::fix(v));
+  } else {
+    atomicOr(status, 1);
+  }
+}
+
 template <typename F, int... Is>
 __device__ __forceinline__ void unroll19_impl(F&& f, std::integer_sequence<int, Is...>) {
   (f(std::integral_constant<int, Is>{}), ...);
@@ -132,46 +171,45 @@ __device__ __forceinline__ void unroll19(F&& f) {
   unroll19_impl(f, std::make_integer_sequence<int, 19>{});
 }
 
-// ---- k_phase: calmacros (Source1.f90:770-831) on the fused state ------------------
-// rr_old / rr_new (16-bit storage only, else null): the reference densities
-// the populations were encoded with, and this step's densities (written with
-// their periodic ghost images like phi) for the encoders of this step.
+// ---- calmacros (Source1.f90:770-831) on the fused state ---------------------------
+// From the accumulated colour densities (the steady-state phase field):
+// phi = (rhoR - rhoB) / rho on fluid nodes, 0 on solid nodes, written with its
+// periodic ghost images; the accumulators are cleared for the collide kernel
+// of this step.  16-bit storage also records rho (rho0 on solid nodes) in
+// rr_new: the reference density this step's encoders use and the next step
+// decodes with.
 template <typename S, bool SOLID>
-__device__ __forceinline__ void phase_node(const DevParams& P, const Pad& pd, const S* __restrict__ pops,
-                                           typename Codec<S>::R* __restrict__ phi,
-                                           const int32_t* __restrict__ walls_all, long long L,
-                                           const float* __restrict__ rr_old, float* __restrict__ rr_new) {
+__device__ __forceinline__ void finalize_node(const DevParams& P, const Pad& pd,
+                                              typename Acc<typename Codec<S>::R>::T* acc,
+                                              typename Codec<S>::R* __restrict__ phi,
+                                              const int32_t* __restrict__ walls_all, float* __restrict__ rr_new,
+                                              const int* __restrict__ status, long long L) {
   using R = typename Codec<S>::R;
+  using A = Acc<R>;
   if (L >= P.N) return;
   // 32-bit index arithmetic (the fused path keeps 38*N < 2^32)
   const unsigned Lu = (unsigned)L, q = Lu / (unsigned)P.nz;
   const int z = (int)(Lu - q * (unsigned)P.nz), x = (int)(q / (unsigned)P.ny), y = (int)(q - (unsigned)x * P.ny);
+  const R sr = A::val(acc[L]), sb = A::val(acc[L + P.N]);
+  acc[L] = 0;
+  acc[L + P.N] = 0;
   R v = R(0);
   R rho = R(P.rho0);
   if (!(SOLID && walls_all[L] >= 1)) {
-    const unsigned N = (unsigned)P.N;
-    const R rref = Codec<S>::kRef ? R(rr_old[pd.idx(x, y, z)]) : R(P.rho0);
-    R sr = R(0), sb = R(0);
-    unroll19([&](auto ic) {
-      constexpr int i = decltype(ic)::value;
-      R r, b;
-      Codec<S>::template load<i>(pops, N, (unsigned)L, rref, r, b);
-      sr = sr + r;
-      sb = sb + b;
-    });
     rho = sr + sb;
     v = (sr - sb) / rho;
   }
+  if (*status) v = R(NAN);
   phi_store<R>(P, pd, phi, x, y, z, v);
   if (Codec<S>::kRef) phi_store<float>(P, pd, rr_new, x, y, z, float(rho));
 }
 
 template <typename S, bool SOLID>
-__global__ void __launch_bounds__(256) k_phase(DevParams P, Pad pd, const S* __restrict__ pops,
-                                               typename Codec<S>::R* __restrict__ phi,
-                                               const int32_t* __restrict__ walls_all, const float* __restrict__ rr_old,
-                                               float* __restrict__ rr_new) {
-  phase_node<S, SOLID>(P, pd, pops, phi, walls_all, blockIdx.x * 256LL + threadIdx.x, rr_old, rr_new);
+__global__ void __launch_bounds__(256) k_finalize(DevParams P, Pad pd, typename Acc<typename Codec<S>::R>::T* acc,
+                                                  typename Codec<S>::R* __restrict__ phi,
+                                                  const int32_t* __restrict__ walls_all, float* __restrict__ rr_new,
+                                                  const int* __restrict__ status) {
+  finalize_node<S, SOLID>(P, pd, acc, phi, walls_all, rr_new, status, blockIdx.x * 256LL + threadIdx.x);
 }
 
 // ---- wetting rotation of a node normal (derivatives :535-587) ---------------------
@@ -203,7 +241,14 @@ struct Smem {
   R phi[5][BY + 4][BZ + 4];
   R n[4][4][BY + 2][BZ + 2];   // [plane][nx,ny,nz,|grad|][y][z]
   float irr[Codec<S>::kRef ? kIrrRing : 1][BY + 4][BZ + 4];   // 1/rho_ref of this step (16-bit storage)
+  R xch[3][2][2][BY][BZ];   // [cx+1][to row y+1, y-1][colour]: density sums crossing rows
 };
+// push order of the collide kernel: groups of equal (cx, cy), cz = 0, +1, -1
+// last (velocity numbering of Source1.f90:132-134)
+__host__ __device__ __forceinline__ constexpr int PUSH_ORDER(int k) {
+  constexpr int a[19] = {0, 5, 6, 1, 11, 13, 2, 12, 14, 3, 15, 17, 4, 16, 18, 7, 8, 9, 10};
+  return a[k];
+}
 
 // One tile: the 32(z) x 8(y) footprint at (z0, y0), planes xa..xb-1.  Called
 // by the single-domain kernel (tile from blockIdx) and by the batched
@@ -216,6 +261,7 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
                                              const int32_t* __restrict__ pout,
                                              const sym_particles* __restrict__ Sp, double* __restrict__ ffi,
                                              const float* __restrict__ rr_old, const float* __restrict__ rr_new,
+                                             typename Acc<typename Codec<S>::R>::T* acc, int* status,
                                              int z0, int y0, int xa, int xb, Smem<S>& sm) {
   using R = typename Codec<S>::R;
   constexpr bool REF = Codec<S>::kRef;
@@ -289,27 +335,54 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
   __syncthreads();
 
   const int y = y0 + ty, z = z0 + tz;
+  const bool inr = y < P.ny && z < P.nz;
+  // every lane runs the node arithmetic (lanes outside the domain on a
+  // clamped node), so the warp shuffles of the density accumulation below see
+  // the whole warp; `act` masks the stores and contributions
+  const int yc = min(y, P.ny - 1), zc = min(z, P.nz - 1);
+  // pushes whose destination lies outside this CTA's tile (or across a
+  // periodic wrap) are added to the accumulators directly; the others are
+  // combined inside the CTA first (z through warp shuffles, y through shared
+  // memory, x in registers along the march) and added once per node
+  const bool ezp = tz == BZ - 1 || z >= P.nz - 1, ezm = tz == 0 || z == 0;
+  const bool eyp = ty == BY - 1 || y >= P.ny - 1, eym = ty == 0 || y == 0;
+  using AT = typename Acc<R>::T;
+  AT* const accR = acc;
+  AT* const accB = acc + N;
+  R aPr = R(0), aPb = R(0), aCr = R(0), aCb = R(0), aNr = R(0), aNb = R(0);   // planes x-1, x, x+1
   for (int x = xa; x < xb; x++) {
     // normals of plane x+1 (phi planes x..x+2 are resident) and phi of plane x+3
     compute_n(x + 1);
     if (x + 3 <= xb + 1) load_phi(x + 3);
     __syncthreads();
-    if (y >= P.ny || z >= P.nz) continue;
-    const unsigned L = (unsigned)(z + sy * y + sx * x);
+    const unsigned L = (unsigned)(zc + sy * yc + sx * x);
+    int pp = 0;
+    bool act = inr;
+    if (SOLID) {
+      if (walls_all[L] > 0) act = false;
+      else pp = pout[L];
+    }
+    // g[cx+1][cy+1][colour]: in-tile pushes summed per destination column and
+    // plane (cz = +-1 pushes arrive from the neighbouring lanes); sf: links
+    // bounced back into this node
+    R g[3][3][2];
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+      for (int b = 0; b < 3; b++)
+#pragma unroll
+        for (int c = 0; c < 2; c++) g[a][b][c] = R(0);
+    R sfr = R(0), sfb = R(0);
+    if (__any_sync(0xffffffffu, act)) {
     if (x + 1 < xb) {
       // bring the next plane's populations toward L2 while this plane computes
 #pragma unroll
       for (int i = 0; i < 19; i++) asm volatile("prefetch.global.L2 [%0];" ::"l"(pin_ + 2 * (i * N + L + sx)));
     }
-    int pp = 0;
-    if (SOLID) {
-      if (walls_all[L] > 0) continue;
-      pp = pout[L];
-    }
     // calmacros on the own populations
     R f[19];
     R sr = R(0), sb = R(0);
-    const R rref = REF ? R(rr_old[pd.idx(x, y, z)]) : R(P.rho0);
+    const R rref = REF ? R(rr_old[pd.idx(x, yc, zc)]) : R(P.rho0);
     unroll19([&](auto ic) {
       constexpr int i = decltype(ic)::value;
       R r, b;
@@ -366,53 +439,133 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
     // post-collision populations for the momentum exchange (:1241-1243), read
     // only next to particles (pout = particle id); wall planes (ids > par)
     // need none, and a handle without particles holds no ffi array
-    if (SOLID && pp >= 1 && pp <= P.par) {
+    if (SOLID && act && pp >= 1 && pp <= P.par) {
 #pragma unroll
       for (int i = 0; i < 19; i++) ffi[(size_t)i * N + L] = (double)f[i];
     }
-    // Latva-Kokko recolouring (:712-726) and push streaming with bounce-back
-    const R ratio = sr * irho;
-    const R coef = sr * sb * irho * R(P.beta);
+    // Latva-Kokko recolouring (:712-726): r_i = (rhoR/rho) f_i + beta rhoR rhoB /
+    // rho w_i (n.c_i); a colour at or below EVAP_LIM empties (r_i = 0 when
+    // rhoR is, r_i = f_i when rhoB is, the latter taking precedence), which the
+    // two coefficients express once per node
     const bool rzero = sr <= evap, bzero = sb <= evap;
+    const R ratio = bzero ? R(1) : (rzero ? R(0) : sr * irho);
+    const R coef = (bzero || rzero || !flag) ? R(0) : sr * sb * irho * R(P.beta);
+    const bool exp_ = x == xb - 1, exm = x == xa;
     // neighbour offsets with the periodic wrap folded in (one select per face)
     const int oxp = (x == P.nx - 1) ? -(P.nx - 1) * sx : sx, oxm = (x == 0) ? (P.nx - 1) * sx : -sx;
-    const int oyp = (y == P.ny - 1) ? -(P.ny - 1) * sy : sy, oym = (y == 0) ? (P.ny - 1) * sy : -sy;
-    const int ozp = (z == P.nz - 1) ? -(P.nz - 1) : 1, ozm = (z == 0) ? (P.nz - 1) : -1;
-    unroll19([&](auto ic) {
-      constexpr int i = decltype(ic)::value;
-      R r = ratio * f[i];
-      if (i > 0 && flag) r = r + coef * R(W(i)) * (nx * R(CX(i)) + ny * R(CY(i)) + nz * R(CZ(i)));
-      if (rzero) r = R(0);
-      if (bzero) r = f[i];
-      const unsigned T = L + (CX(i) > 0 ? oxp : (CX(i) < 0 ? oxm : 0)) + (CY(i) > 0 ? oyp : (CY(i) < 0 ? oym : 0)) +
-                         (CZ(i) > 0 ? ozp : (CZ(i) < 0 ? ozm : 0));
-      if (SOLID && i > 0 && pp >= 1) {
-        const int wb = walls[T];
-        const bool flat = wb > P.par;
-        if (wb == pp || flat) {
-          // curve (:1001-1019): link OPC(i) of this node comes back reversed
-          constexpr int j = OPC(i);
-          R star = R(0);
-          if (!flat) {
-            const int par = P.par;
-            const R xr = R(disp(P, (double)(x + P.origin), Sp->center[0 * par + wb - 1], 0));
-            const R yr = R(disp(P, (double)(y + P.origin), Sp->center[1 * par + wb - 1], 1));
-            const R zr = R(disp(P, (double)(z + P.origin), Sp->center[2 * par + wb - 1], 2));
-            const R uw0 = R(Sp->up[0 * par + wb - 1]) + zr * R(Sp->rp[1 * par + wb - 1]) - yr * R(Sp->rp[2 * par + wb - 1]);
-            const R uw1 = R(Sp->up[1 * par + wb - 1]) + xr * R(Sp->rp[2 * par + wb - 1]) - zr * R(Sp->rp[0 * par + wb - 1]);
-            const R uw2 = R(Sp->up[2 * par + wb - 1]) + yr * R(Sp->rp[0 * par + wb - 1]) - xr * R(Sp->rp[1 * par + wb - 1]);
-            star = uw0 * R(CX(j)) + uw1 * R(CY(j)) + uw2 * R(CZ(j));
+    const int oyp = (yc == P.ny - 1) ? -(P.ny - 1) * sy : sy, oym = (yc == 0) ? (P.ny - 1) * sy : -sy;
+    const int ozp = (zc == P.nz - 1) ? -(P.nz - 1) : 1, ozm = (zc == 0) ? (P.nz - 1) : -1;
+    R zp[2] = {R(0), R(0)}, zm[2] = {R(0), R(0)};
+    // directions in groups of equal (cx, cy): within a group only cz differs,
+    // and the cz = +-1 pushes of the group move one lane up / down right after it
+    static_for<19>([&](auto kc) {
+      constexpr int k = decltype(kc)::value;
+      constexpr int i = PUSH_ORDER(k);
+      constexpr int a = CX(i) + 1, b = CY(i) + 1;
+      [&] {
+        R r = ratio * f[i];
+        if (i > 0) r = r + coef * R(W(i)) * (nx * R(CX(i)) + ny * R(CY(i)) + nz * R(CZ(i)));
+        const unsigned T = L + (CX(i) > 0 ? oxp : (CX(i) < 0 ? oxm : 0)) +
+                           (CY(i) > 0 ? oyp : (CY(i) < 0 ? oym : 0)) + (CZ(i) > 0 ? ozp : (CZ(i) < 0 ? ozm : 0));
+        if (!act) return;
+        if (SOLID && i > 0 && pp >= 1) {
+          const int wb = walls[T];
+          const bool flat = wb > P.par;
+          if (wb == pp || flat) {
+            // curve (:1001-1019): link OPC(i) of this node comes back reversed
+            constexpr int j = OPC(i);
+            R star = R(0);
+            if (!flat) {
+              const int par = P.par;
+              const R xr = R(disp(P, (double)(x + P.origin), Sp->center[0 * par + wb - 1], 0));
+              const R yr = R(disp(P, (double)(y + P.origin), Sp->center[1 * par + wb - 1], 1));
+              const R zr = R(disp(P, (double)(z + P.origin), Sp->center[2 * par + wb - 1], 2));
+              const R uw0 = R(Sp->up[0 * par + wb - 1]) + zr * R(Sp->rp[1 * par + wb - 1]) -
+                            yr * R(Sp->rp[2 * par + wb - 1]);
+              const R uw1 = R(Sp->up[1 * par + wb - 1]) + xr * R(Sp->rp[2 * par + wb - 1]) -
+                            zr * R(Sp->rp[0 * par + wb - 1]);
+              const R uw2 = R(Sp->up[2 * par + wb - 1]) + yr * R(Sp->rp[0 * par + wb - 1]) -
+                            xr * R(Sp->rp[1 * par + wb - 1]);
+              star = uw0 * R(CX(j)) + uw1 * R(CY(j)) + uw2 * R(CZ(j));
+            }
+            const R rr = r + R(6.0 * W(j)) * sr * star;
+            const R bb = (f[i] - r) + R(6.0 * W(j)) * sb * star;
+            const R irr = REF ? R(sm.irr[x % kIrrRing][ty + 2][tz + 2]) : irho0;
+            Codec<S>::template store<j>(pout_, N, L, irr, rr, rr + bb);
+            sfr = sfr + rr;
+            sfb = sfb + bb;
+            return;
           }
-          const R rr = r + R(6.0 * W(j)) * sr * star;
-          const R bb = (f[i] - r) + R(6.0 * W(j)) * sb * star;
-          const R irr = REF ? R(sm.irr[x % kIrrRing][ty + 2][tz + 2]) : irho0;
-          Codec<S>::template store<j>(pout_, N, L, irr, rr, rr + bb);
-          return;
+        }
+        const R irr = REF ? R(sm.irr[(x + CX(i) + kIrrRing) % kIrrRing][ty + 2 + CY(i)][tz + 2 + CZ(i)]) : irho0;
+        Codec<S>::template store<i>(pout_, N, T, irr, r, f[i]);
+        const R bv = f[i] - r;
+        const bool ext = (CX(i) > 0 && exp_) || (CX(i) < 0 && exm) || (CY(i) > 0 && eyp) || (CY(i) < 0 && eym) ||
+                         (CZ(i) > 0 && ezp) || (CZ(i) < 0 && ezm);
+        if (ext) {
+          acc_add<R>(accR + T, r, status);
+          acc_add<R>(accB + T, bv, status);
+        } else if (CZ(i) == 0) {
+          g[a][b][0] = g[a][b][0] + r;
+          g[a][b][1] = g[a][b][1] + bv;
+        } else if (CZ(i) > 0) {
+          zp[0] = r;
+          zp[1] = bv;
+        } else {
+          zm[0] = r;
+          zm[1] = bv;
+        }
+      }();
+      if constexpr (CZ(i) < 0) {
+        // last of a group with cz = 0, +1, -1: lane l receives the cz = +1 push
+        // of lane l-1 and the cz = -1 push of lane l+1 (lane = tz)
+#pragma unroll
+        for (int c = 0; c < 2; c++) {
+          const R up = __shfl_up_sync(0xffffffffu, zp[c], 1);
+          const R dn = __shfl_down_sync(0xffffffffu, zm[c], 1);
+          g[a][b][c] = g[a][b][c] + (tz > 0 ? up : R(0)) + (tz < BZ - 1 ? dn : R(0));
+          zp[c] = R(0);
+          zm[c] = R(0);
         }
       }
-      const R irr = REF ? R(sm.irr[(x + CX(i) + kIrrRing) % kIrrRing][ty + 2 + CY(i)][tz + 2 + CZ(i)]) : irho0;
-      Codec<S>::template store<i>(pout_, N, T, irr, r, f[i]);
     });
+    }
+    // along y through shared memory: row ty+1 receives the cy = +1 sums of row
+    // ty and row ty-1 the cy = -1 sums, for each destination plane
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        sm.xch[a][0][c][ty][tz] = g[a][2][c];
+        sm.xch[a][1][c][ty][tz] = g[a][0][c];
+      }
+    __syncthreads();
+    R in[3][2];
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        R v = g[a][1][c];
+        if (ty > 0) v = v + sm.xch[a][0][c][ty - 1][tz];
+        if (ty < BY - 1) v = v + sm.xch[a][1][c][ty + 1][tz];
+        in[a][c] = v;
+      }
+    aPr = aPr + in[0][0]; aPb = aPb + in[0][1];
+    aCr = aCr + in[1][0] + sfr; aCb = aCb + in[1][1] + sfb;
+    aNr = aNr + in[2][0]; aNb = aNb + in[2][1];
+    // plane x-1 of this column has all its in-tile contributions
+    if (x > xa && inr && (aPr != R(0) || aPb != R(0))) {
+      acc_add<R>(accR + (L - sx), aPr, status);
+      acc_add<R>(accB + (L - sx), aPb, status);
+    }
+    aPr = aCr; aPb = aCb;
+    aCr = aNr; aCb = aNb;
+    aNr = R(0); aNb = R(0);
+  }
+  if (xb > xa && inr && (aPr != R(0) || aPb != R(0))) {
+    const unsigned L = (unsigned)(z + sy * y + sx * (xb - 1));
+    acc_add<R>(accR + L, aPr, status);
+    acc_add<R>(accB + L, aPb, status);
   }
 }
 
@@ -431,12 +584,13 @@ __global__ void __launch_bounds__(TPB, collide_ctas<S>()) k_collide(DevParams P,
                                                    const int32_t* __restrict__ pout,
                                                    const sym_particles* __restrict__ Sp, double* __restrict__ ffi,
                                                    const float* __restrict__ rr_old, const float* __restrict__ rr_new,
+                                                   typename Acc<typename Codec<S>::R>::T* acc, int* status,
                                                    int xchunk) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem<S>& sm = *reinterpret_cast<Smem<S>*>(smem_raw);
   const int xa = blockIdx.z * xchunk;
-  collide_tile<S, SOLID>(P, pd, pin_, pout_, phi, walls, walls_all, pout, Sp, ffi, rr_old, rr_new, blockIdx.x * BZ,
-                         blockIdx.y * BY, xa, min(xa + xchunk, P.nx), sm);
+  collide_tile<S, SOLID>(P, pd, pin_, pout_, phi, walls, walls_all, pout, Sp, ffi, rr_old, rr_new, acc, status,
+                         blockIdx.x * BZ, blockIdx.y * BY, xa, min(xa + xchunk, P.nx), sm);
 }
 
 // ---- pin fill on the fused state (derivatives :467-492) ----------------------------
@@ -584,12 +738,13 @@ __global__ void k_fast_refill_import(DevParams P, Pad pd, int n, double margin, 
 // reference its populations are encoded with (a solid or empty node keeps rho0)
 template <typename S>
 __global__ void k_import_pops(DevParams P, Pad pd, const double* __restrict__ ri, const double* __restrict__ bi,
-                              S* pops, float* rr) {
+                              S* pops, float* rr, typename Acc<typename Codec<S>::R>::T* acc, int* status) {
   using R = typename Codec<S>::R;
   const long long L = blockIdx.x * 256LL + threadIdx.x;
   if (L >= P.N) return;
   const unsigned N = (unsigned)P.N;
   R irr = R(1.0 / P.rho0);
+  R sr = R(0), sb = R(0);
   if (Codec<S>::kRef) {
     double rho = 0.0;
     for (int i = 0; i < 19; i++) rho += ri[(size_t)i * N + L] + bi[(size_t)i * N + L];
@@ -603,7 +758,14 @@ __global__ void k_import_pops(DevParams P, Pad pd, const double* __restrict__ ri
     constexpr int i = decltype(ic)::value;
     const R r = R(ri[(size_t)i * N + L]), b = R(bi[(size_t)i * N + L]);
     Codec<S>::template store<i>(pops, N, (unsigned)L, irr, r, r + b);
+    sr = sr + r;
+    sb = sb + b;
   });
+  // the accumulators the first phase field after the import reads
+  using A = Acc<R>;
+  if (!A::ok(sr) || !A::ok(sb)) atomicOr(status, 1);
+  acc[L] = A::ok(sr) ? A::fix(sr) : 0;
+  acc[L + P.N] = A::ok(sb) ? A::fix(sb) : 0;
 }
 template <typename S>
 __global__ void k_export_pops(DevParams P, Pad pd, const S* __restrict__ pops, const float* __restrict__ rr, double* ri,

@@ -19,6 +19,8 @@ struct FastState {
   double* phi[2] = {nullptr, nullptr};  // FP64 halo-padded phase field (pin-filled)
   float* phif[2] = {nullptr, nullptr};  // FP32 halo-padded phase field for FP32/FP16 storage
   float* rref[2] = {nullptr, nullptr};  // 16-bit storage: halo-padded reference densities (same parity as phi)
+  void* acc = nullptr;     // next step's colour densities, fixed point [red N][blue N] (see fused.cuh)
+  int* status = nullptr;   // sticky: bit 0 an accumulated density was not finite or out of range
   bool valid = false;      // fast state holds the authoritative populations
   size_t bytes = 0;
   cudaGraph_t graph[2] = {nullptr, nullptr};       // one captured step per buffer parity
