@@ -235,11 +235,17 @@ __device__ __forceinline__ void wet_rotate(const DevParams& P, const sym_particl
 // (phi x+4 -> slot (x-1)%5, normals x+2 -> (x-2)%4, 1/rho_ref x+4 -> (x-2)%6)
 // are never among them.
 constexpr int kIrrRing = 6;
+// unit normal and |grad phi| of one node, read with one (FP32) or two (FP64)
+// 16-byte shared-memory accesses
+template <typename R>
+struct alignas(4 * sizeof(R)) NormalV {
+  R x, y, z, g;
+};
 template <typename S>
 struct Smem {
   using R = typename Codec<S>::R;
   R phi[5][BY + 4][BZ + 4];
-  R n[4][4][BY + 2][BZ + 2];   // [plane][nx,ny,nz,|grad|][y][z]
+  NormalV<R> n[4][BY + 2][BZ + 2];   // [plane][y][z]: n and |grad phi|
   float irr[Codec<S>::kRef ? kIrrRing : 1][BY + 4][BZ + 4];   // 1/rho_ref of this step (16-bit storage)
   R xch[3][2][2][BY][BZ];   // [cx+1][to row y+1, y-1][colour]: density sums crossing rows
 };
@@ -304,14 +310,17 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
         else pp = pout[Lw];
       }
       if (ok) {
+        // grad phi = 3 sum_i w_i c_i phi(x + c_i) (:510-521), summed over the
+        // nine opposite pairs: w_i c_i (phi(x + c_i) - phi(x - c_i))
         R g0 = R(0), g1 = R(0), g2 = R(0);
-#pragma unroll
-        for (int i = 1; i < 19; i++) {
-          const R val = R(W(i)) * sm.phi[(((xp + CX(i)) % 5) + 5) % 5][py + 1 + CY(i)][pz + 1 + CZ(i)];
-          if (CX(i)) g0 = g0 + val * R(CX(i));
-          if (CY(i)) g1 = g1 + val * R(CY(i));
-          if (CZ(i)) g2 = g2 + val * R(CZ(i));
-        }
+        static_for<9>([&](auto kc) {
+          constexpr int i = PREP(decltype(kc)::value);
+          const R d = sm.phi[(((xp + CX(i)) % 5) + 5) % 5][py + 1 + CY(i)][pz + 1 + CZ(i)] -
+                      sm.phi[(((xp - CX(i)) % 5) + 5) % 5][py + 1 - CY(i)][pz + 1 - CZ(i)];
+          if (CX(i)) g0 = g0 + R(W(i) * CX(i)) * d;
+          if (CY(i)) g1 = g1 + R(W(i) * CY(i)) * d;
+          if (CZ(i)) g2 = g2 + R(W(i) * CZ(i)) * d;
+        });
         g0 = R(3) * g0; g1 = R(3) * g1; g2 = R(3) * g2;
         fn = sqrt(g0 * g0 + g1 * g1 + g2 * g2);
         if (fn > evap) {
@@ -322,7 +331,7 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
           fn = R(0);
         }
       }
-      sm.n[s][0][py][pz] = n0; sm.n[s][1][py][pz] = n1; sm.n[s][2][py][pz] = n2; sm.n[s][3][py][pz] = fn;
+      sm.n[s][py][pz] = NormalV<R>{n0, n1, n2, fn};
     }
   };
 
@@ -402,25 +411,25 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
     const R irho = R(1) / rho;
     ux = ux * irho; uy = uy * irho; uz = uz * irho;
     const int s1 = x % 4;
-    const R nx = sm.n[s1][0][ty + 1][tz + 1], ny = sm.n[s1][1][ty + 1][tz + 1], nz = sm.n[s1][2][ty + 1][tz + 1];
-    const R fn = sm.n[s1][3][ty + 1][tz + 1];
+    const NormalV<R> nown = sm.n[s1][ty + 1][tz + 1];
+    const R nx = nown.x, ny = nown.y, nz = nown.z, fn = nown.g;
     const bool flag = fn > evap;
     const R rhoN = sm.phi[x % 5][ty + 2][tz + 2];
     // CSF surface tension from the curvature of the normal field (:624-667)
     R fx = R(0), fy = R(0), fz = R(0);
     if (flag && (!SOLID || pp <= 0)) {
+      // d_ba = sum_i w_i c_ia n_b(x + c_i) (:635-660), over the nine opposite
+      // pairs: w_i c_ia (n_b(x + c_i) - n_b(x - c_i))
       R d00 = 0, d01 = 0, d02 = 0, d10 = 0, d11 = 0, d12 = 0, d20 = 0, d21 = 0, d22 = 0;
-#pragma unroll
-      for (int i = 1; i < 19; i++) {
-        const int sl = (x + CX(i) + 4) % 4;
-        const int yy = ty + 1 + CY(i), zz = tz + 1 + CZ(i);
-        const R a = R(W(i)) * sm.n[sl][0][yy][zz];
-        const R b = R(W(i)) * sm.n[sl][1][yy][zz];
-        const R c = R(W(i)) * sm.n[sl][2][yy][zz];
-        if (CX(i)) { d00 = d00 + a * R(CX(i)); d10 = d10 + b * R(CX(i)); d20 = d20 + c * R(CX(i)); }
-        if (CY(i)) { d01 = d01 + a * R(CY(i)); d11 = d11 + b * R(CY(i)); d21 = d21 + c * R(CY(i)); }
-        if (CZ(i)) { d02 = d02 + a * R(CZ(i)); d12 = d12 + b * R(CZ(i)); d22 = d22 + c * R(CZ(i)); }
-      }
+      static_for<9>([&](auto kc) {
+        constexpr int i = PREP(decltype(kc)::value);
+        const NormalV<R> p = sm.n[(x + CX(i) + 4) % 4][ty + 1 + CY(i)][tz + 1 + CZ(i)];
+        const NormalV<R> m = sm.n[(x - CX(i) + 4) % 4][ty + 1 - CY(i)][tz + 1 - CZ(i)];
+        const R a = p.x - m.x, b = p.y - m.y, c = p.z - m.z;
+        if (CX(i)) { constexpr double k = W(i) * CX(i); d00 = d00 + R(k) * a; d10 = d10 + R(k) * b; d20 = d20 + R(k) * c; }
+        if (CY(i)) { constexpr double k = W(i) * CY(i); d01 = d01 + R(k) * a; d11 = d11 + R(k) * b; d21 = d21 + R(k) * c; }
+        if (CZ(i)) { constexpr double k = W(i) * CZ(i); d02 = d02 + R(k) * a; d12 = d12 + R(k) * b; d22 = d22 + R(k) * c; }
+      });
       d00 *= R(3); d01 *= R(3); d02 *= R(3); d10 *= R(3); d11 *= R(3); d12 *= R(3);
       d20 *= R(3); d21 *= R(3); d22 *= R(3);
       const R kurv = nx * ny * (d10 + d01) + nx * nz * (d20 + d02) + ny * nz * (d12 + d21) -

@@ -260,6 +260,9 @@ __host__ __device__ __forceinline__ constexpr bool MEVEN(int r) {
   return true;
 }
 
+// rows relaxed with the fixed rate 1 (density, momentum)
+__host__ __device__ __forceinline__ constexpr bool MCONS(int r) { return r == 0 || r == 3 || r == 5 || r == 7; }
+
 template <int... Is, typename F>
 __device__ __forceinline__ void static_for_impl(F&& f, std::integer_sequence<int, Is...>) {
   (f(std::integral_constant<int, Is>{}), ...);
@@ -287,6 +290,7 @@ __device__ __forceinline__ void mrt_collide_pairs(const DevParams& P, R f[19], R
     constexpr int r = decltype(rc)::value;
     constexpr bool even = MEVEN(r);
     R acc = R(0);
+    if constexpr (MCONS(r)) return;   // relaxed with rate 1: not needed (below)
     if constexpr (even && MROW(r, 0) != 0.0) acc = R(MROW(r, 0)) * f[0];
     static_for<9>([&](auto kc) {
       constexpr int k = decltype(kc)::value;
@@ -301,8 +305,12 @@ __device__ __forceinline__ void mrt_collide_pairs(const DevParams& P, R f[19], R
   R meq[19], fk[19];
   equilf<R, false>(meq, fk, rho, ux, uy, uz, fx, fy, fz);
   const R s[19] = {R(1), se, seps, R(1), sq, R(1), sq, R(1), sq, su, spi, su, spi, su, su, su, sm, sm, sm};
-#pragma unroll
-  for (int k = 0; k < 19; k++) m[k] = m[k] - s[k] * (m[k] - meq[k]) + (R(1) - R(0.5) * s[k]) * fk[k];
+  // density and momentum relax with rate 1 (:684): m - (m - meq) + fk/2 = meq + fk/2
+  static_for<19>([&](auto kc) {
+    constexpr int k = decltype(kc)::value;
+    if constexpr (MCONS(k)) m[k] = meq[k] + R(0.5) * fk[k];
+    else m[k] = m[k] - s[k] * (m[k] - meq[k]) + (R(1) - R(0.5) * s[k]) * fk[k];
+  });
   {
     R e = R(0);
     static_for<19>([&](auto rc) {
