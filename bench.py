@@ -392,6 +392,8 @@ def main():
                     help="auxiliary measurements at N=1 (comma list; 'none' for the timed region only)")
     ap.add_argument("--domains", type=int, default=96, help="mix: the first D domains of the manifest "
                                                              "(smaller cases for profiler captures)")
+    ap.add_argument("--xchunk", type=int, default=0, help="mix: fixed tile x extent for every domain instead of "
+                                                           "the autotuner (profiler captures)")
     ap.add_argument("--serve-seconds", type=float, default=20.0)
     ap.add_argument("--serve-cap", type=int, default=300)
     ap.add_argument("--serve-wall", type=float, default=75.0)
@@ -440,7 +442,12 @@ def mix_main(args, torch, dist, rank, world, local, legs, peak, peak_kind):
     nodes = sum(w.nodes for w in ws)
     lattices = [setup_workload(w, device=local) for w in ws]
     B = Batch(lattices)
-    tuned_steps = B.autotune(trial_steps=3)
+    if args.xchunk > 0:
+        for i in range(len(ws)):
+            B.set_xchunk(i, args.xchunk)
+        tuned_steps = 0
+    else:
+        tuned_steps = B.autotune(trial_steps=3)
     cls = lambda nx: 0 if nx <= 32 else (1 if nx <= 48 else 2)  # noqa: E731
     xchunk = {}
     for i, w in enumerate(ws):

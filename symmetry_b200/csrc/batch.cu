@@ -43,6 +43,8 @@ struct DomainDesc {
   float* rr_new;
   void* acc;            // accumulated colour densities of the next step (see fused.cuh)
   int* status;
+  const CUtensorMap* tm_phi;    // TMA descriptors (device copies) of this step's phase field
+  const CUtensorMap* tm_rinv;   // and 1/rho_ref arrays
   int solid;
   int pad_;
 };
@@ -73,10 +75,12 @@ __global__ void __launch_bounds__(kTPB, collide_ctas<S>()) k_collide_batch(const
                                                            const TileEntry* __restrict__ tiles, int ntiles,
                                                            int* __restrict__ counter) {
   using R = typename Codec<S>::R;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  Smem<S>& sm = *reinterpret_cast<Smem<S>*>(smem_raw);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  Smem<S>& sm = smem_view<S>(smem_raw);
   __shared__ int s_tile;
   __shared__ __align__(16) DomainDesc s_desc;
+  collide_init_barriers<S>(sm);
+  unsigned nload = 0;
   for (;;) {
     if (threadIdx.x == 0) s_tile = atomicAdd(counter, 1);
     __syncthreads();
@@ -93,11 +97,12 @@ __global__ void __launch_bounds__(kTPB, collide_ctas<S>()) k_collide_batch(const
     using AT = typename Acc<R>::T;
     if (D.solid)
       collide_tile<S, true>(D.P, D.pd, (const S*)D.pin, (S*)D.pnext, (const R*)D.phic, D.walls, D.walls_all, D.pout,
-                            D.Sp, D.ffi, D.rr_old, D.rr_new, (AT*)D.acc, D.status, e.z0, e.y0, e.xa, e.xb, sm);
+                            D.Sp, D.ffi, D.rr_old, D.rr_new, (AT*)D.acc, D.status, D.tm_phi, D.tm_rinv, e.z0,
+                            e.y0, e.xa, e.xb, sm, nload);
     else
       collide_tile<S, false>(D.P, D.pd, (const S*)D.pin, (S*)D.pnext, (const R*)D.phic, D.walls, D.walls_all,
-                             D.pout, D.Sp, D.ffi, D.rr_old, D.rr_new, (AT*)D.acc, D.status, e.z0, e.y0, e.xa, e.xb,
-                             sm);
+                             D.pout, D.Sp, D.ffi, D.rr_old, D.rr_new, (AT*)D.acc, D.status, D.tm_phi, D.tm_rinv,
+                             e.z0, e.y0, e.xa, e.xb, sm, nload);
     __syncthreads();
   }
 }
@@ -105,7 +110,7 @@ __global__ void __launch_bounds__(kTPB, collide_ctas<S>()) k_collide_batch(const
 template <typename S>
 int set_batch_smem(cudaStream_t, int* grid_blocks, int device) {
   using R = typename Codec<S>::R;
-  const int shm = (int)sizeof(Smem<S>);
+  const int shm = (int)smem_bytes<S>();
   if (cudaFuncSetAttribute(k_collide_batch<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, shm) != cudaSuccess)
     return SYM_ERR_CUDA;
   int per_sm = 0, sms = 0;
@@ -126,6 +131,7 @@ struct sym_batch {
   std::vector<int> built_cur, built_pc;   // domain parities graph 0 was built for
   int steps_since_build = 0;
   DomainDesc* d_desc[2] = {nullptr, nullptr};
+  CUtensorMap* d_tmaps = nullptr;   // [parity][domain][phase field, 1/rho_ref]
   int2* d_blk = nullptr;          // phase block -> (domain, block in domain)
   TileEntry* d_tiles = nullptr;
   int ntiles = 0;
@@ -171,6 +177,7 @@ void free_tables(sym_batch* b) {
     if (b->d_desc[k]) { cudaFree(b->d_desc[k]); b->d_desc[k] = nullptr; }
   if (b->d_blk) { cudaFree(b->d_blk); b->d_blk = nullptr; }
   if (b->d_tiles) { cudaFree(b->d_tiles); b->d_tiles = nullptr; }
+  if (b->d_tmaps) { cudaFree(b->d_tmaps); b->d_tmaps = nullptr; }
 }
 
 void* popp(sym_handle* h, int k) { return h->fast.pop[k]; }
@@ -260,8 +267,8 @@ int enqueue_batch_step(sym_batch* b, int k, cudaEvent_t* ev) {
   if (ev) cudaEventRecord(ev[2], b->st);
   cudaMemsetAsync(b->d_counter + k, 0, sizeof(int), b->st);
   using R = typename Codec<S>::R;
-  k_collide_batch<S><<<b->grid, kTPB, sizeof(Smem<S>), b->st>>>(b->d_desc[k], b->d_tiles, b->ntiles,
-                                                                 b->d_counter + k);
+  k_collide_batch<S><<<b->grid, kTPB, smem_bytes<S>(), b->st>>>(b->d_desc[k], b->d_tiles, b->ntiles,
+                                                                  b->d_counter + k);
   if (ev) cudaEventRecord(ev[3], b->st);
   return bcuda(b, cudaGetLastError(), "batch step");
 }
@@ -307,6 +314,19 @@ int build(sym_batch* b) {
   std::stable_sort(tiles.begin(), tiles.end(), [](const TileEntry& a, const TileEntry& c) { return a.cost > c.cost; });
   b->ntiles = (int)tiles.size();
   b->nblocks = off[n];
+  // TMA descriptors: the device copies the domain descriptors point at
+  std::vector<CUtensorMap> maps((size_t)4 * n);
+  if (int e = bcuda(b, cudaMalloc(&b->d_tmaps, sizeof(CUtensorMap) * maps.size()), "descriptor maps")) return e;
+  for (int k = 0; k < 2; k++)
+    for (int i = 0; i < n; i++) {
+      const int pc = (b->built_pc[i] + k) & 1;
+      const size_t j = ((size_t)k * n + i) * 2;
+      maps[j] = b->doms[i]->fast.tm_phi[pc];
+      maps[j + 1] = b->doms[i]->fast.tm_rinv[pc];
+      desc[k][i].tm_phi = b->d_tmaps + j;
+      desc[k][i].tm_rinv = b->d_tmaps + j + 1;
+    }
+  cudaMemcpyAsync(b->d_tmaps, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice, b->st);
   for (int k = 0; k < 2; k++) {
     if (int e = bcuda(b, cudaMalloc(&b->d_desc[k], sizeof(DomainDesc) * n), "descriptors")) return e;
     cudaMemcpyAsync(b->d_desc[k], desc[k].data(), sizeof(DomainDesc) * n, cudaMemcpyHostToDevice, b->st);

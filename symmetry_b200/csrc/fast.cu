@@ -26,6 +26,7 @@
 #include <cuda_fp16.h>
 #include <cmath>
 #include <cstdio>
+#include <mutex>
 #include <utility>
 #include <vector>
 #include "state.cuh"
@@ -142,23 +143,25 @@ int enqueue_step(sym_handle* h, int cur, int pc, cudaEvent_t* ev) {
   // (a3-a9) fused derivatives + collision + recolour + stream + bounce-back
   const int xc = h->fast.xchunk > 0 ? h->fast.xchunk : XCHUNK;
   dim3 grid((P.nz + BZ - 1) / BZ, (P.ny + BY - 1) / BY, (P.nx + xc - 1) / xc);
-  const size_t shm = sizeof(Smem<S>);
+  const size_t shm = smem_bytes<S>();
+  const CUtensorMap& tp = h->fast.tm_phi[pc];
+  const CUtensorMap& tr = h->fast.tm_rinv[pc];
   if (ev) cudaEventRecord(ev[2], h->st);
   if (solid)
     k_collide<S, true><<<grid, TPB, shm, h->st>>>(P, pd, pin_, pnext, phic, h->walls, h->walls_all, h->pout,
                                                   h->dpart, h->ffi, rr_old(h, pc), rr_new(h, pc), accbuf<S>(h),
-                                                  h->fast.status, xc);
+                                                  h->fast.status, tp, tr, xc);
   else
     k_collide<S, false><<<grid, TPB, shm, h->st>>>(P, pd, pin_, pnext, phic, h->walls, h->walls_all, h->pout,
                                                    h->dpart, h->ffi, rr_old(h, pc), rr_new(h, pc), accbuf<S>(h),
-                                                   h->fast.status, xc);
+                                                   h->fast.status, tp, tr, xc);
   if (ev) cudaEventRecord(ev[3], h->st);
   return check_cuda(h, cudaGetLastError(), "fast step");
 }
 
 template <typename S>
 int set_smem_attr(sym_handle* h) {
-  const int shm = (int)sizeof(Smem<S>);
+  const int shm = (int)smem_bytes<S>();
   cudaError_t e = cudaFuncSetAttribute(k_collide<S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, shm);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_collide<S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, shm);
@@ -233,6 +236,20 @@ int fast_alloc(sym_handle* h) {
   if (int e = dev_carve(h, (void**)&F.status, sizeof(int))) return e;
   if (h->planning) return SYM_OK;
   F.bytes = h->bytes - before;
+  // TMA descriptors of the phase-field (and 16-bit 1/rho_ref) tiles the
+  // collide kernel reads: boxes of (BZ+4) x (BY+4) x 1 over the padded arrays
+  for (int k = 0; k < 2; k++) {
+    const bool f64 = F.storage == SYM_STORE_FP64;
+    void* phi = f64 ? (void*)F.phi[k] : (void*)F.phif[k];
+    if (tma::encode_padded(&F.tm_phi[k], phi, f64 ? 8 : 4, h->dp.nz + 4, pd.nzp, pd.nyp, pd.nxp, BZ + 4, BY + 4))
+      return set_error(h, SYM_ERR_CUDA, "TMA descriptor of the phase field");
+    if (F.storage == SYM_STORE_FP16) {
+      if (tma::encode_padded(&F.tm_rinv[k], F.rref[k], 4, h->dp.nz + 4, pd.nzp, pd.nyp, pd.nxp, BZ + 4, BY + 4))
+        return set_error(h, SYM_ERR_CUDA, "TMA descriptor of the reference densities");
+    } else {
+      F.tm_rinv[k] = F.tm_phi[k];   // not read
+    }
+  }
   return F.storage == SYM_STORE_FP64 ? set_smem_attr<double>(h)
        : F.storage == SYM_STORE_FP32 ? set_smem_attr<float>(h) : set_smem_attr<__half>(h);
 }
@@ -368,6 +385,36 @@ int fast_step_timed(sym_handle* h, int nsteps, double ms[4]) {
   for (auto& e : ev) cudaEventDestroy(e);
   return rc;
 }
+
+namespace tma {
+int encode_padded(CUtensorMap* map, void* base, int esize, int nz_ext, int nzp, int nyp, int nxp, int box_z,
+                  int box_y) {
+  static PFN_cuTensorMapEncodeTiled encode = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled>(fn);
+  });
+  if (!encode) return SYM_ERR_CUDA;
+  // the rules a tiled TMA load relies on: 16-byte base and pitches, an inner
+  // box extent that is a whole number of 16-byte units, at most 256 per box side
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || ((size_t)nzp * esize) % 16 || ((size_t)box_z * esize) % 16 ||
+      box_z > 256 || box_y > 256 || nz_ext > nzp)
+    return SYM_ERR_PARAM;
+  const cuuint64_t dims[3] = {(cuuint64_t)nz_ext, (cuuint64_t)nyp, (cuuint64_t)nxp};
+  const cuuint64_t strides[2] = {(cuuint64_t)nzp * esize, (cuuint64_t)nzp * nyp * esize};
+  const cuuint32_t box[3] = {(cuuint32_t)box_z, (cuuint32_t)box_y, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = encode(map, esize == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                            base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? SYM_OK : SYM_ERR_CUDA;
+}
+}  // namespace tma
 
 }  // namespace symb200
 

@@ -6,6 +6,7 @@
 #include <cmath>
 #include <utility>
 #include "state.cuh"
+#include "tma.cuh"
 
 namespace symb200 {
 namespace fused {
@@ -175,9 +176,9 @@ __device__ __forceinline__ void unroll19(F&& f) {
 // From the accumulated colour densities (the steady-state phase field):
 // phi = (rhoR - rhoB) / rho on fluid nodes, 0 on solid nodes, written with its
 // periodic ghost images; the accumulators are cleared for the collide kernel
-// of this step.  16-bit storage also records rho (rho0 on solid nodes) in
+// of this step.  16-bit storage also records 1/rho (1/rho0 on solid nodes) in
 // rr_new: the reference density this step's encoders use and the next step
-// decodes with.
+// decodes with (rr_new here, rr_old there: both hold 1/rho_ref).
 template <typename S, bool SOLID>
 __device__ __forceinline__ void finalize_node(const DevParams& P, const Pad& pd,
                                               typename Acc<typename Codec<S>::R>::T* acc,
@@ -201,7 +202,7 @@ __device__ __forceinline__ void finalize_node(const DevParams& P, const Pad& pd,
   }
   if (*status) v = R(NAN);
   phi_store<R>(P, pd, phi, x, y, z, v);
-  if (Codec<S>::kRef) phi_store<float>(P, pd, rr_new, x, y, z, float(rho));
+  if (Codec<S>::kRef) phi_store<float>(P, pd, rr_new, x, y, z, 1.0f / float(rho));
 }
 
 template <typename S, bool SOLID>
@@ -241,14 +242,38 @@ template <typename R>
 struct alignas(4 * sizeof(R)) NormalV {
   R x, y, z, g;
 };
+// phi and 1/rho_ref plane tiles ((BY+4) x (BZ+4), z fastest) arrive by TMA:
+// each slot starts on a 128-byte boundary
+constexpr int kPlaneTile = (BY + 4) * (BZ + 4);
 template <typename S>
 struct Smem {
   using R = typename Codec<S>::R;
-  R phi[5][BY + 4][BZ + 4];
+  static constexpr int kPhiSlot = (kPlaneTile * (int)sizeof(R) + 127) / 128 * 128 / (int)sizeof(R);
+  static constexpr int kIrrSlot = (kPlaneTile * 4 + 127) / 128 * 128 / 4;
+  alignas(128) R phi[5][kPhiSlot];
+  alignas(128) float irr[Codec<S>::kRef ? kIrrRing : 1][kIrrSlot];   // 1/rho_ref of this step (16-bit storage)
   NormalV<R> n[4][BY + 2][BZ + 2];   // [plane][y][z]: n and |grad phi|
-  float irr[Codec<S>::kRef ? kIrrRing : 1][BY + 4][BZ + 4];   // 1/rho_ref of this step (16-bit storage)
   R xch[3][2][2][BY][BZ];   // [cx+1][to row y+1, y-1][colour]: density sums crossing rows
+  uint64_t bar[kIrrRing];   // one mbarrier per plane load, used round robin
 };
+// dynamic shared memory of the collide kernels: the Smem block on a 128-byte
+// boundary inside the allocation
+template <typename S>
+constexpr size_t smem_bytes() { return sizeof(Smem<S>) + 128; }
+template <typename S>
+__device__ __forceinline__ Smem<S>& smem_view(unsigned char* raw) {
+  const uintptr_t a = (reinterpret_cast<uintptr_t>(raw) + 127) & ~uintptr_t(127);
+  return *reinterpret_cast<Smem<S>*>(a);
+}
+// the CTA's mbarriers: initialised once per kernel by thread 0
+template <typename S>
+__device__ __forceinline__ void collide_init_barriers(Smem<S>& sm) {
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < kIrrRing; k++) tma::mbar_init(&sm.bar[k], 1);
+    tma::mbar_fence_init();
+  }
+  __syncthreads();
+}
 // push order of the collide kernel: groups of equal (cx, cy), cz = 0, +1, -1
 // last (velocity numbering of Source1.f90:132-134)
 __host__ __device__ __forceinline__ constexpr int PUSH_ORDER(int k) {
@@ -268,7 +293,8 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
                                              const sym_particles* __restrict__ Sp, double* __restrict__ ffi,
                                              const float* __restrict__ rr_old, const float* __restrict__ rr_new,
                                              typename Acc<typename Codec<S>::R>::T* acc, int* status,
-                                             int z0, int y0, int xa, int xb, Smem<S>& sm) {
+                                             const CUtensorMap* tm_phi, const CUtensorMap* tm_rinv,
+                                             int z0, int y0, int xa, int xb, Smem<S>& sm, unsigned& nload) {
   using R = typename Codec<S>::R;
   constexpr bool REF = Codec<S>::kRef;
   const int tz = threadIdx.x % BZ, ty = threadIdx.x / BZ;
@@ -277,24 +303,26 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
   const R evap = R(P.evap);
   const int sy = P.nz, sx = P.nz * P.ny;   // element strides of y and x
 
-  // load phi plane xp (padded coordinates stay inside the ghost layers)
-  auto load_phi = [&](int xp) {
-    const int sl = ((xp % 5) + 5) % 5;
-    R(*dst)[BZ + 4] = sm.phi[sl];
-    for (int t = threadIdx.x; t < (BY + 4) * (BZ + 4); t += TPB) {
-      const int py = t / (BZ + 4), pz = t % (BZ + 4);
-      const int y = y0 - 2 + py, z = z0 - 2 + pz;
-      R v = R(0);
-      float ir = 1.0f;
-      if (y <= P.ny + 1 && z <= P.nz + 1) {
-        const long long q = pd.idx(xp, y, z);
-        v = phi[q];
-        if (REF) ir = 1.0f / rr_new[q];
-      }
-      dst[py][pz] = v;
-      if (REF) sm.irr[((xp % kIrrRing) + kIrrRing) % kIrrRing][py][pz] = ir;
-    }
+  // phi (and 1/rho_ref) of plane xp by TMA: one box of (BY+4) x (BZ+4) at the
+  // padded origin (z0, y0, xp+2) -- z0 is a multiple of 32 elements, so the
+  // innermost coordinate is 128-byte aligned; rows past the padded extent read
+  // as zeros.  Plane xp is load number nl0 + xp - (xa - 2) of this CTA, on
+  // mbarrier (number mod 6) with phase parity (number / 6) mod 2.
+  const unsigned nl0 = nload;
+  auto load_no = [&](int xp) { return nl0 + (unsigned)(xp - (xa - 2)); };
+  constexpr uint32_t kTx = kPlaneTile * (sizeof(R) + (REF ? 4 : 0));
+  auto load_phi = [&](int xp) {   // thread 0 only
+    const unsigned q = load_no(xp);
+    uint64_t* bar = &sm.bar[q % kIrrRing];
+    tma::mbar_expect_tx(bar, kTx);
+    tma::load_3d(sm.phi[((xp % 5) + 5) % 5], tm_phi, z0, y0, xp + 2, bar);
+    if (REF) tma::load_3d(sm.irr[((xp % kIrrRing) + kIrrRing) % kIrrRing], tm_rinv, z0, y0, xp + 2, bar);
   };
+  auto wait_phi = [&](int xp) {   // every thread
+    const unsigned q = load_no(xp);
+    if (!tma::mbar_wait(&sm.bar[q % kIrrRing], (q / kIrrRing) & 1u)) atomicOr(status, 2);
+  };
+  auto PHI = [&](int xp, int py, int pz) -> R { return sm.phi[((xp % 5) + 5) % 5][py * (BZ + 4) + pz]; };
   // unit normal (rotated at wetting nodes) and |grad phi| of plane xp, halo 1
   auto compute_n = [&](int xp) {
     const int s = ((xp % 4) + 4) % 4;
@@ -315,8 +343,7 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
         R g0 = R(0), g1 = R(0), g2 = R(0);
         static_for<9>([&](auto kc) {
           constexpr int i = PREP(decltype(kc)::value);
-          const R d = sm.phi[(((xp + CX(i)) % 5) + 5) % 5][py + 1 + CY(i)][pz + 1 + CZ(i)] -
-                      sm.phi[(((xp - CX(i)) % 5) + 5) % 5][py + 1 - CY(i)][pz + 1 - CZ(i)];
+          const R d = PHI(xp + CX(i), py + 1 + CY(i), pz + 1 + CZ(i)) - PHI(xp - CX(i), py + 1 - CY(i), pz + 1 - CZ(i));
           if (CX(i)) g0 = g0 + R(W(i) * CX(i)) * d;
           if (CY(i)) g1 = g1 + R(W(i) * CY(i)) * d;
           if (CZ(i)) g2 = g2 + R(W(i) * CZ(i)) * d;
@@ -335,13 +362,15 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
     }
   };
 
-  load_phi(xa - 2); load_phi(xa - 1); load_phi(xa); load_phi(xa + 1); load_phi(xa + 2);
-  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int xp = xa - 2; xp <= xa + 2; xp++) load_phi(xp);
+  for (int xp = xa - 2; xp <= xa + 2; xp++) wait_phi(xp);
   compute_n(xa - 1);
   compute_n(xa);
   // the first iteration's phi load reuses the slot of plane xa-2, which
   // compute_n(xa-1) above reads
   __syncthreads();
+  nload = nl0 + (unsigned)(xb - xa + 4);   // loads of this tile: planes xa-2 .. xb+1
 
   const int y = y0 + ty, z = z0 + tz;
   const bool inr = y < P.ny && z < P.nz;
@@ -360,9 +389,12 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
   AT* const accB = acc + N;
   R aPr = R(0), aPb = R(0), aCr = R(0), aCb = R(0), aNr = R(0), aNb = R(0);   // planes x-1, x, x+1
   for (int x = xa; x < xb; x++) {
-    // normals of plane x+1 (phi planes x..x+2 are resident) and phi of plane x+3
+    // phi of plane x+3 on its way; normals of plane x+1 from phi planes x..x+2.
+    // The slots the load overwrites (phi of plane x-2, 1/rho_ref of plane x-3)
+    // were last read before the previous plane's barriers.
+    if (threadIdx.x == 0 && x + 3 <= xb + 1) load_phi(x + 3);
+    wait_phi(x + 2);
     compute_n(x + 1);
-    if (x + 3 <= xb + 1) load_phi(x + 3);
     __syncthreads();
     const unsigned L = (unsigned)(zc + sy * yc + sx * x);
     int pp = 0;
@@ -391,7 +423,7 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
     // calmacros on the own populations
     R f[19];
     R sr = R(0), sb = R(0);
-    const R rref = REF ? R(rr_old[pd.idx(x, yc, zc)]) : R(P.rho0);
+    const R rref = REF ? R(1) / R(rr_old[pd.idx(x, yc, zc)]) : R(P.rho0);
     unroll19([&](auto ic) {
       constexpr int i = decltype(ic)::value;
       R r, b;
@@ -414,7 +446,7 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
     const NormalV<R> nown = sm.n[s1][ty + 1][tz + 1];
     const R nx = nown.x, ny = nown.y, nz = nown.z, fn = nown.g;
     const bool flag = fn > evap;
-    const R rhoN = sm.phi[x % 5][ty + 2][tz + 2];
+    const R rhoN = PHI(x, ty + 2, tz + 2);
     // CSF surface tension from the curvature of the normal field (:624-667)
     R fx = R(0), fy = R(0), fz = R(0);
     if (flag && (!SOLID || pp <= 0)) {
@@ -499,14 +531,15 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
             }
             const R rr = r + R(6.0 * W(j)) * sr * star;
             const R bb = (f[i] - r) + R(6.0 * W(j)) * sb * star;
-            const R irr = REF ? R(sm.irr[x % kIrrRing][ty + 2][tz + 2]) : irho0;
+            const R irr = REF ? R(sm.irr[x % kIrrRing][(ty + 2) * (BZ + 4) + tz + 2]) : irho0;
             Codec<S>::template store<j>(pout_, N, L, irr, rr, rr + bb);
             sfr = sfr + rr;
             sfb = sfb + bb;
             return;
           }
         }
-        const R irr = REF ? R(sm.irr[(x + CX(i) + kIrrRing) % kIrrRing][ty + 2 + CY(i)][tz + 2 + CZ(i)]) : irho0;
+        const R irr =
+            REF ? R(sm.irr[(x + CX(i) + kIrrRing) % kIrrRing][(ty + 2 + CY(i)) * (BZ + 4) + tz + 2 + CZ(i)]) : irho0;
         Codec<S>::template store<i>(pout_, N, T, irr, r, f[i]);
         const R bv = f[i] - r;
         const bool ext = (CX(i) > 0 && exp_) || (CX(i) < 0 && exm) || (CY(i) > 0 && eyp) || (CY(i) < 0 && eym) ||
@@ -594,12 +627,15 @@ __global__ void __launch_bounds__(TPB, collide_ctas<S>()) k_collide(DevParams P,
                                                    const sym_particles* __restrict__ Sp, double* __restrict__ ffi,
                                                    const float* __restrict__ rr_old, const float* __restrict__ rr_new,
                                                    typename Acc<typename Codec<S>::R>::T* acc, int* status,
-                                                   int xchunk) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  Smem<S>& sm = *reinterpret_cast<Smem<S>*>(smem_raw);
+                                                   const __grid_constant__ CUtensorMap tm_phi,
+                                                   const __grid_constant__ CUtensorMap tm_rinv, int xchunk) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  Smem<S>& sm = smem_view<S>(smem_raw);
+  collide_init_barriers<S>(sm);
+  unsigned nload = 0;
   const int xa = blockIdx.z * xchunk;
   collide_tile<S, SOLID>(P, pd, pin_, pout_, phi, walls, walls_all, pout, Sp, ffi, rr_old, rr_new, acc, status,
-                         blockIdx.x * BZ, blockIdx.y * BY, xa, min(xa + xchunk, P.nx), sm);
+                         &tm_phi, &tm_rinv, blockIdx.x * BZ, blockIdx.y * BY, xa, min(xa + xchunk, P.nx), sm, nload);
 }
 
 // ---- pin fill on the fused state (derivatives :467-492) ----------------------------
@@ -678,7 +714,7 @@ __global__ void k_fast_prep(DevParams P, Pad pd, int n, double margin, int pp, c
   if (!fbox_node(P, n, margin, Sp->center, pp, blockIdx.x * (long long)blockDim.x + threadIdx.x, x, y, z)) return;
   const long long L = lin(P, x, y, z);
   const unsigned N = (unsigned)P.N;
-  const R rref = Codec<S>::kRef ? R(rr_old[pd.idx(x, y, z)]) : R(P.rho0);
+  const R rref = Codec<S>::kRef ? R(1) / R(rr_old[pd.idx(x, y, z)]) : R(P.rho0);
   if (walls_all[L] > 0) {
     rhoN[L] = 0.0;
     gx[L] = 0.0; gy[L] = 0.0; gz[L] = 0.0; nxv[L] = 0.0; nyv[L] = 0.0; nzv[L] = 0.0;
@@ -733,7 +769,7 @@ __global__ void k_fast_refill_import(DevParams P, Pad pd, int n, double margin, 
   const unsigned N = (unsigned)P.N;
   if (pout[L] != pp || walls_old[L] < 1) return;
   // the collide of this step decodes these populations with rr_old
-  const R irr = Codec<S>::kRef ? R(1) / R(rr_old[pd.idx(x, y, z)]) : R(1.0 / P.rho0);
+  const R irr = Codec<S>::kRef ? R(rr_old[pd.idx(x, y, z)]) : R(1.0 / P.rho0);
   unroll19([&](auto ic) {
     constexpr int i = decltype(ic)::value;
     const R r = R(ri[(size_t)i * N + L]), b = R(bi[(size_t)i * N + L]);
@@ -760,8 +796,8 @@ __global__ void k_import_pops(DevParams P, Pad pd, const double* __restrict__ ri
     const float ref = rho > 0.0 ? float(rho) : float(P.rho0);
     const unsigned Lu = (unsigned)L, q = Lu / (unsigned)P.nz;
     const int z = (int)(Lu - q * (unsigned)P.nz), x = (int)(q / (unsigned)P.ny), y = (int)(q - (unsigned)x * P.ny);
-    phi_store<float>(P, pd, rr, x, y, z, ref);
     irr = R(1) / R(ref);
+    phi_store<float>(P, pd, rr, x, y, z, float(irr));
   }
   unroll19([&](auto ic) {
     constexpr int i = decltype(ic)::value;
@@ -787,7 +823,7 @@ __global__ void k_export_pops(DevParams P, Pad pd, const S* __restrict__ pops, c
   if (Codec<S>::kRef) {
     const unsigned Lu = (unsigned)L, q = Lu / (unsigned)P.nz;
     const int z = (int)(Lu - q * (unsigned)P.nz), x = (int)(q / (unsigned)P.ny), y = (int)(q - (unsigned)x * P.ny);
-    rref = R(rr[pd.idx(x, y, z)]);
+    rref = R(1) / R(rr[pd.idx(x, y, z)]);
   }
   unroll19([&](auto ic) {
     constexpr int i = decltype(ic)::value;

@@ -1,5 +1,6 @@
 // state.cuh -- device state behind a sym_handle.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <string>
 #include "../../include/symmetry.h"
@@ -18,9 +19,13 @@ struct FastState {
   int xchunk = 0;          // x planes per tile of the fused collide kernel (0 = default)
   double* phi[2] = {nullptr, nullptr};  // FP64 halo-padded phase field (pin-filled)
   float* phif[2] = {nullptr, nullptr};  // FP32 halo-padded phase field for FP32/FP16 storage
-  float* rref[2] = {nullptr, nullptr};  // 16-bit storage: halo-padded reference densities (same parity as phi)
+  float* rref[2] = {nullptr, nullptr};  // 16-bit storage: halo-padded 1/rho_ref (same parity as phi)
   void* acc = nullptr;     // next step's colour densities, fixed point [red N][blue N] (see fused.cuh)
-  int* status = nullptr;   // sticky: bit 0 an accumulated density was not finite or out of range
+  int* status = nullptr;   // sticky: bit 0 an accumulated density was not finite or out of
+                           // range, bit 1 a shared-memory tile load did not complete in time
+  // TMA descriptors of the halo-padded phase field and 1/rho_ref arrays, per parity
+  CUtensorMap tm_phi[2] = {};
+  CUtensorMap tm_rinv[2] = {};
   bool valid = false;      // fast state holds the authoritative populations
   size_t bytes = 0;
   cudaGraph_t graph[2] = {nullptr, nullptr};       // one captured step per buffer parity
