@@ -210,29 +210,55 @@ def cpu_baseline(samples, label, budget_s=20.0):
                       "(g++ -O3 -fopenmp), not the Fortran binary (no Fortran compiler on this image)"}
 
 
+def cpu_run_each(samples, warmup, steps):
+    """Each domain in turn through the oracle (all host threads): set up,
+    `warmup` untimed steps, `steps` timed steps, freed before the next one (the
+    whole mix at once would hold ~40 GB of host memory).  Returns (node updates
+    per step over all domains, seconds per step over all domains)."""
+    from oracle import oracle as orc
+    nodes, sec = 0, 0.0
+    for w in samples:
+        o = orc.setup_workload(w)
+        for _ in range(warmup):
+            o.step(1)
+        t0 = time.perf_counter()
+        o.step(steps)
+        sec += (time.perf_counter() - t0) / steps
+        nodes += w.params.n_nodes
+        del o
+    return nodes, sec
+
+
 def run_reference(args):
     """--impl reference: the reference's algorithm on the host cores (the oracle
-    port; the Fortran reference cannot be compiled on this image), on a
-    bounded sample of the same workload."""
+    port; the Fortran reference cannot be compiled on this image).  The mix
+    runs every one of its domains (the GPU arm's configuration), one domain
+    at a time."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     from oracle import oracle as orc
     if args.workload == "mix":
-        samples, label, cfg = mix_sample(4), "the first 4 domains of the batched mix", MIX_DESC
+        from symmetry_b200 import configs
+        samples = configs.c4_manifest(storage="fp64")[:max(1, min(96, args.domains))]
+        label = f"all {len(samples)} domains of the batched mix, one at a time"
+        cfg = MIX_DESC + ("" if len(samples) == 96 else f" (first {len(samples)} domains only)")
+        nodes, sec = cpu_run_each(samples, args.warmup, args.steps)
+        same = len(samples) == 96
     else:
         w = workload(args.workload, "fp64", args.size)
         samples, label, cfg = thread_sample(w), "a z-slab of the domain", describe(w, "fp64")
-    nodes, sec, n = cpu_run(samples, args.warmup, steps=args.steps)
+        nodes, sec, n = cpu_run(samples, args.warmup, steps=args.steps)
+        same = False
     v = nodes / sec / 1e6
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "MLUPS", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded phase fields)",
-        "config": {"workload": cfg, "sample_nodes_per_step": nodes},
+        "config": {"workload": cfg, "nodes_per_step": nodes, "same_config_as_gpu_arm": same},
         "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": orc.threads(), "kind": "port",
-                         "sample": f"{label}, {nodes} nodes per step; C++ restatement of Source1.f90 "
-                                   "(no Fortran compiler on this image)"},
+                         "sample": f"{label}, {nodes} nodes per step, {args.steps} timed steps each; C++ "
+                                   "restatement of Source1.f90 (no Fortran compiler on this image)"},
         "e2e": {"value": v, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -245,11 +271,12 @@ def pinned(torch, shape):
     return torch.empty(n, dtype=torch.float64, pin_memory=True).numpy().reshape(shape)
 
 
-def e2e_batch(torch, lattices, B, inner=100):
+def e2e_batch(torch, lattices, B, inner=100, reps=3):
     """End to end through the C ABI with pinned host buffers, one output
     interval of the reference driver: upload ri, bi and rho_N of every domain
-    (Fortran layout), `inner` batch steps, calmacros and download rho_N, rho,
-    ux, uy, uz of every domain."""
+    (Fortran layout), `inner` batch steps, then calmacros of every domain
+    downloaded as rho_N, rho, ux, uy, uz (sym_get_macros); `reps` timed
+    intervals after one warm-up interval."""
     host = []
     h2d = d2h = 0
     for L in lattices:
@@ -270,16 +297,18 @@ def e2e_batch(torch, lattices, B, inner=100):
             L.set_populations(ri, bi)
         B.step(inner)
         for L, (ri, bi, phi, outs) in zip(lattices, host):
-            L.call("calmacros")
-            for name, o in zip(["rho_N", "rho", "ux", "uy", "uz"], outs):
-                L.get_into(name, o)
+            L.macros(dict(zip(["rho_N", "rho", "ux", "uy", "uz"], outs)))
 
     one()   # warm-up (graph rebuild after the uploads)
-    t0 = time.perf_counter()
-    one()
-    dt = time.perf_counter() - t0
+    dts = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        one()
+        dts.append(time.perf_counter() - t0)
+    dt = sum(dts) / len(dts)
     return {"value": nodes * inner / dt / 1e6, "unit": "MLUPS", "h2d_bytes_per_step": h2d / inner,
-            "d2h_bytes_per_step": d2h / inner, "inner_steps": inner,
+            "d2h_bytes_per_step": d2h / inner, "inner_steps": inner, "repeats": reps,
+            "interval_s": {"mean": dt, "min": min(dts), "max": max(dts)},
             "step": f"upload ri+bi+rho_N of all 96 domains (pinned, Fortran layout, {h2d / 1e9:.2f} GB) -> "
                     f"{inner} batch steps -> calmacros -> download rho_N,rho,u ({d2h / 1e9:.2f} GB); "
                     "per-step bytes = interval bytes / inner steps"}

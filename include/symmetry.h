@@ -150,6 +150,13 @@ int sym_get_field(sym_handle* h, int field, void* host);
 /* Upload both colours' populations (0:18,z,y,x) in one call: the state a
  * Fortran driver holds after initialization (Source1.f90:883-894). */
 int sym_set_populations(sym_handle* h, const double* ri, const double* bi);
+/* The macroscopic fields calmacros (Source1.f90:770-831) computes from the
+ * current populations -- rho, ux, uy, uz and rho_N, each (z,y,x) -- without
+ * changing the stepping state (the fields an output step of the reference
+ * driver writes, :218-234).  On a handle stepped by sym_step the fused state
+ * stays authoritative, so reading does not re-encode reduced storage.  Any
+ * pointer may be NULL. */
+int sym_get_macros(sym_handle* h, double* rho, double* ux, double* uy, double* uz, double* rho_n);
 int sym_set_particles(sym_handle* h, const sym_particles* s);
 int sym_get_particles(sym_handle* h, sym_particles* s);
 /* Lagrange point arrays (par, La_num) column-major as in :1805; any pointer may be NULL. */

@@ -421,6 +421,20 @@ int sym_get_field(sym_handle* h, int field, void* host) {
   return check_cuda(h, cudaStreamSynchronize(h->st), "get_field");
 }
 
+int sym_get_macros(sym_handle* h, double* rho, double* ux, double* uy, double* uz, double* rho_n) {
+  if (int e = guard(h)) return e;
+  if (h->fast.valid) {
+    if (int e = fast_macros(h)) return e;
+  } else {
+    if (int e = ref_calmacros(h)) return e;
+  }
+  double* src[5] = {h->rho, h->ux, h->uy, h->uz, h->rhoN};
+  double* dst[5] = {rho, ux, uy, uz, rho_n};
+  for (int k = 0; k < 5; k++)
+    if (dst[k]) cudaMemcpyAsync(dst[k], src[k], sizeof(double) * h->N, cudaMemcpyDeviceToHost, h->st);
+  return check_cuda(h, cudaStreamSynchronize(h->st), "get_macros");
+}
+
 int sym_set_populations(sym_handle* h, const double* ri, const double* bi) {
   if (int e = guard(h)) return e;
   if (!ri || !bi) return set_error(h, SYM_ERR_PARAM, "null populations");

@@ -328,6 +328,28 @@ int fast_export(sym_handle* h) {
   return check_cuda(h, cudaStreamSynchronize(h->st), "fast export");
 }
 
+// calmacros of the current fused populations into the canonical macro arrays
+// (rho, u, rho_N), leaving the fused state authoritative
+int fast_macros(sym_handle* h) {
+  FastState& F = h->fast;
+  const DevParams& P = h->dp;
+  const Pad pd = make_pad(P);
+  switch (F.storage) {
+    case SYM_STORE_FP64:
+      k_macros<double><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, popbuf<double>(h, F.cur), nullptr, h->walls_all,
+                                                           h->rho, h->ux, h->uy, h->uz, h->rhoN);
+      break;
+    case SYM_STORE_FP32:
+      k_macros<float><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, popbuf<float>(h, F.cur), nullptr, h->walls_all,
+                                                          h->rho, h->ux, h->uy, h->uz, h->rhoN);
+      break;
+    default:
+      k_macros<__half><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, popbuf<__half>(h, F.cur), F.rref[1 - F.pc],
+                                                           h->walls_all, h->rho, h->ux, h->uy, h->uz, h->rhoN);
+  }
+  return check_cuda(h, cudaGetLastError(), "fast macros");
+}
+
 // nsteps fused steps; each parity (which population/phi buffer is current) has
 // its own captured graph
 int fast_step(sym_handle* h, int nsteps) {

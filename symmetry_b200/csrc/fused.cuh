@@ -833,6 +833,46 @@ __global__ void k_export_pops(DevParams P, Pad pd, const S* __restrict__ pops, c
     bi[(size_t)i * N + L] = (double)b;
   });
 }
+// calmacros (Source1.f90:770-831) of the current fused populations without
+// touching the fused state: rho, u = sum f c / rho (no force shift) and
+// phi = (rhoR - rhoB) / rho on fluid nodes; phi = 0, u = 0, rho = rho0 on
+// solid nodes.  rr (16-bit storage): 1/rho_ref of the populations.
+template <typename S>
+__global__ void k_macros(DevParams P, Pad pd, const S* __restrict__ pops, const float* __restrict__ rr,
+                         const int32_t* __restrict__ walls_all, double* rho, double* ux, double* uy, double* uz,
+                         double* rhoN) {
+  using R = typename Codec<S>::R;
+  const long long L = blockIdx.x * 256LL + threadIdx.x;
+  if (L >= P.N) return;
+  if (walls_all[L] >= 1) {
+    rhoN[L] = 0.0; ux[L] = 0.0; uy[L] = 0.0; uz[L] = 0.0; rho[L] = P.rho0;
+    return;
+  }
+  const unsigned N = (unsigned)P.N;
+  R rref = R(P.rho0);
+  if (Codec<S>::kRef) {
+    const unsigned Lu = (unsigned)L, q = Lu / (unsigned)P.nz;
+    const int z = (int)(Lu - q * (unsigned)P.nz), x = (int)(q / (unsigned)P.ny), y = (int)(q - (unsigned)x * P.ny);
+    rref = R(1) / R(rr[pd.idx(x, y, z)]);
+  }
+  double sr = 0.0, sb = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
+  unroll19([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    R r, b;
+    Codec<S>::template load<i>(pops, N, (unsigned)L, rref, r, b);
+    const double f = (double)r + (double)b;
+    sr += (double)r;
+    sb += (double)b;
+    if (CX(i)) mx += f * CX(i);
+    if (CY(i)) my += f * CY(i);
+    if (CZ(i)) mz += f * CZ(i);
+  });
+  const double rh = sr + sb;
+  rho[L] = rh;
+  ux[L] = mx / rh; uy[L] = my / rh; uz[L] = mz / rh;
+  rhoN[L] = (sr - sb) / rh;
+}
+
 template <typename R>
 __global__ void k_import_phi(DevParams P, Pad pd, const double* __restrict__ rhoN, R* phi) {
   const long long L = blockIdx.x * 256LL + threadIdx.x;

@@ -112,6 +112,7 @@ int fast_alloc(sym_handle* h);
 void fast_free(sym_handle* h);
 int fast_import(sym_handle* h);   // canonical -> fast
 int fast_export(sym_handle* h);   // fast -> canonical
+int fast_macros(sym_handle* h);   // calmacros of the fused populations into rho, u, rho_N (fused state kept)
 int fast_step(sym_handle* h, int nsteps);
 int fast_step_timed(sym_handle* h, int nsteps, double ms[4]);
 int fast_enqueue_sparse(sym_handle* h, int cur, int pc);   // particles + pin fill on h->st

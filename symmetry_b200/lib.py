@@ -58,6 +58,7 @@ def lib() -> ctypes.CDLL:
         L.sym_set_field.argtypes = [H, ctypes.c_int, ctypes.c_void_p]
         L.sym_get_field.argtypes = [H, ctypes.c_int, ctypes.c_void_p]
         L.sym_set_populations.argtypes = [H, ctypes.c_void_p, ctypes.c_void_p]
+        L.sym_get_macros.argtypes = [H] + [ctypes.c_void_p] * 5
         L.sym_set_particles.argtypes = [H, ctypes.POINTER(SymParticles)]
         L.sym_get_particles.argtypes = [H, ctypes.POINTER(SymParticles)]
         L.sym_get_lagrange.argtypes = [H] + [ctypes.c_void_p] * 9
@@ -158,6 +159,20 @@ class Lattice:
         shape = self.shape + ((19,) if name in POP_FIELDS else ())
         out = np.empty(shape, dtype=dt)
         self._ck(lib().sym_get_field(self.h, FIELD_ID[name], out.ctypes.data), f"get {name}")
+        return out
+
+    def macros(self, out: Optional[Dict[str, np.ndarray]] = None) -> Dict[str, np.ndarray]:
+        """rho, ux, uy, uz, rho_N of the current populations (calmacros),
+        without changing the stepping state; `out` may supply the host arrays
+        (contiguous float64 of the domain's size, e.g. pinned)."""
+        names = ("rho", "ux", "uy", "uz", "rho_N")
+        if out is None:
+            out = {k: np.empty(self.shape, dtype=np.float64) for k in names}
+        for k in names:
+            a = out[k]
+            if a.dtype != np.float64 or not a.flags.c_contiguous or a.size != self.p.n_nodes:
+                raise ValueError(f"{k}: contiguous float64 array of {self.p.n_nodes} values expected")
+        self._ck(lib().sym_get_macros(self.h, *(out[k].ctypes.data for k in names)), "get_macros")
         return out
 
     def set_populations(self, ri: np.ndarray, bi: np.ndarray):

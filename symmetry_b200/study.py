@@ -1,19 +1,24 @@
-"""Precision study of the population storage modes on one large domain.
+"""Precision study of the population storage modes.
 
-The 256x256x512 Rayleigh-Plateau thread (R=24, 2% perturbation over one
-512-node wavelength, tau=0.7, sigma=8e-3, beta=0.7, seed 1003) runs in FP64,
-FP32 and FP16 shifted storage side by side, in lockstep, until breakup (the
-minimum over z of r_eq(z) = sqrt(sum_xy (1+phi)/2 / pi) falls below one
-lattice unit, read every 10 steps and linearly interpolated) or the step cap.
-Every `snap_every` steps each reduced mode's density, velocity and phase
-fields are compared with FP64 (relative L2 over the domain; velocity as one
-vector field) and every mode's total mass is compared with its initial value
-(mass drift).  The breakup step of each mode is compared with FP64's.
+Each case runs in FP64, FP32 and 16-bit shifted storage side by side, in
+lockstep, until breakup (the minimum over z of r_eq(z) = sqrt(sum_xy
+(1+phi)/2 / pi) falls below one lattice unit, read every `check` steps and
+linearly interpolated) or the step cap.  Every `snap_every` steps each reduced
+mode's density, velocity and phase fields are compared with FP64 (relative L2
+over the domain; velocity as one vector field) and every mode's total mass is
+compared with its initial value (mass drift).  The breakup step of each mode
+is compared with FP64's.  Snapshots read the macroscopic fields through
+sym_get_macros, which leaves the stepping state untouched (no re-encoding).
 
-  python -m symmetry_b200.study [--max-steps 40000] [--size 256x256x512] [--out study.json]
+Cases:
+  c3       the 256x256x512 Rayleigh-Plateau thread (R=24, 2% perturbation
+           over one 512-node wavelength, tau=0.7, sigma=8e-3, beta=0.7,
+           seed 1003), 40,000-step cap (--size scales it down)
+  mix:K    the first K sphere-free domains of the batched-mix manifest whose
+           wavelength is unstable (lambda > 2 pi R): threads that break within
+           the cap, for the breakup-time error
 
-A snapshot exports the fused state to the canonical arrays, which re-encodes
-the 16-bit populations once: one extra rounding per snapshot interval.
+  python -m symmetry_b200.study [--case c3|mix:K] [--max-steps N] [--size NXxNYxNZ] [--out study.json]
 """
 from __future__ import annotations
 
@@ -28,6 +33,8 @@ import numpy as np
 from . import configs
 from .lib import setup_workload
 
+MODES = ("fp64", "fp32", "fp16")
+
 
 def rel_l2(a, b):
     d = np.linalg.norm((np.asarray(a) - np.asarray(b)).ravel())
@@ -35,19 +42,14 @@ def rel_l2(a, b):
     return float(d / n) if n > 0 else float(d)
 
 
-def snapshot(L):
-    L.call("calmacros")
-    return {k: L.get(k) for k in ("rho", "ux", "uy", "uz", "rho_N")}
+def with_storage(w, mode):
+    p = w.params.copy()
+    p.storage = {"fp64": 0, "fp32": 1, "fp16": 2}[mode]
+    return configs.Workload(w.name, p, w.kind, dict(w.gen), w.steps, list(w.particles))
 
 
-def run(size=None, modes=("fp64", "fp32", "fp16"), max_steps=40000, check=10, snap_every=5000,
-        threshold=1.0, log=sys.stderr):
-    if size:
-        nx, ny, nz = (int(v) for v in size.lower().split("x"))
-        mk = lambda m: configs.c3_thread(nx=nx, ny=ny, nz=nz, storage=m, radius=24.0 * nx / 256.0)  # noqa: E731
-    else:
-        mk = lambda m: configs.c3_thread(storage=m)  # noqa: E731
-    lat = {m: setup_workload(mk(m)) for m in modes}
+def run_case(w, modes=MODES, max_steps=40000, check=10, snap_every=5000, threshold=1.0, log=sys.stderr):
+    lat = {m: setup_workload(with_storage(w, m)) for m in modes}
     mass0 = {}
     for m, L in lat.items():
         mm = L.mass_momentum()
@@ -71,27 +73,30 @@ def run(size=None, modes=("fp64", "fp32", "fp16"), max_steps=40000, check=10, sn
             prev[m] = (s, r)
         t += check
         if t % snap_every == 0 and all(breakup[m] is None for m in modes):
-            ref = snapshot(lat[modes[0]])
+            ref = lat[modes[0]].macros()
             row = {"step": t, "rmin": {m: prev[m][1] for m in modes}}
             for m in modes:
                 mm = lat[m].mass_momentum()
                 row.setdefault("mass_drift", {})[m] = (mm[0] + mm[1] - mass0[m]) / mass0[m]
                 if m == modes[0]:
                     continue
-                sn = snapshot(lat[m])
+                sn = lat[m].macros()
                 u = np.stack([sn[k] for k in ("ux", "uy", "uz")])
                 uref = np.stack([ref[k] for k in ("ux", "uy", "uz")])
                 row.setdefault("l2", {})[m] = {"u": rel_l2(u, uref), "rho": rel_l2(sn["rho"], ref["rho"]),
                                                 "phi": rel_l2(sn["rho_N"], ref["rho_N"])}
             snaps.append(row)
-            print(json.dumps(row), file=log, flush=True)
+            print(json.dumps({"case": w.name, **row}), file=log, flush=True)
     base = breakup[modes[0]]
     out = {
-        "workload": f"c3_thread {mk('fp64').params.nx}x{mk('fp64').params.ny}x{mk('fp64').params.nz}",
+        "case": w.name, "size": [w.params.nx, w.params.ny, w.params.nz], "gen": w.gen,
+        "tau": 3.0 * w.params.nu_r + 0.5, "sigma": w.params.sigma,
         "modes": list(modes), "check_every": check, "threshold": threshold, "max_steps": max_steps,
         "steps_run": t, "wall_s": time.time() - t0, "breakup_step": breakup,
         "breakup_rel_err": {m: (abs(breakup[m] - base) / base if (breakup[m] is not None and base) else None)
                             for m in modes},
+        "max_l2_u": {m: max((r["l2"][m]["u"] for r in snaps), default=None) for m in modes[1:]},
+        "last_l2": snaps[-1]["l2"] if snaps else None,
         "snapshots": snaps,
     }
     for L in lat.values():
@@ -99,19 +104,44 @@ def run(size=None, modes=("fp64", "fp32", "fp16"), max_steps=40000, check=10, sn
     return out
 
 
+def mix_cases(k):
+    """The first k sphere-free manifest domains with an unstable wavelength."""
+    out = []
+    for w in configs.c4_manifest(storage="fp64"):
+        if w.params.par:
+            continue
+        if w.gen["wavelength"] > 2.0 * math.pi * w.gen["radius"]:
+            out.append(w)
+        if len(out) == k:
+            break
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
+    ap.add_argument("--case", default="c3")
     ap.add_argument("--size", default=None)
     ap.add_argument("--max-steps", type=int, default=40000)
     ap.add_argument("--snap-every", type=int, default=5000)
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
-    res = run(size=a.size, max_steps=a.max_steps, snap_every=a.snap_every)
-    s = json.dumps(res)
-    if a.out:
-        with open(a.out, "w") as f:
-            f.write(s + "\n")
-    print(s)
+    if a.case == "c3":
+        if a.size:
+            nx, ny, nz = (int(v) for v in a.size.lower().split("x"))
+            ws = [configs.c3_thread(nx=nx, ny=ny, nz=nz, radius=24.0 * nx / 256.0)]
+        else:
+            ws = [configs.c3_thread()]
+    elif a.case.startswith("mix:"):
+        ws = mix_cases(int(a.case.split(":")[1]))
+    else:
+        raise SystemExit(f"unknown case {a.case}")
+    res = []
+    for w in ws:
+        res.append(run_case(w, max_steps=a.max_steps, snap_every=a.snap_every))
+        if a.out:   # keep what finished if a later case is cut short
+            with open(a.out, "w") as f:
+                f.write(json.dumps(res) + "\n")
+    print(json.dumps(res))
 
 
 if __name__ == "__main__":

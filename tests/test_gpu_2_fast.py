@@ -139,3 +139,31 @@ def test_reduced_storage_early_thread(storage, bound):
     e = errors(o, L, ["ux", "uy", "uz", "rho", "rho_N"])
     print(f"{storage} early thread: {e}")
     assert e["u"] <= bound, e
+
+
+@pytest.mark.parametrize("storage", ["fp64", "fp16"])
+def test_get_macros_leaves_stepping_state_untouched(storage):
+    """sym_get_macros on a fused state returns calmacros of the current
+    populations and changes nothing: a run that reads the fields midway ends
+    bit for bit where an unread run ends, and the fields equal calmacros of
+    the exported populations."""
+    w = configs.c2_wall_particle(nx=24, ny=24, nz=48, rad=4.0, centre=(12.0, 12.0, 16.0), z0=16.0, z1=32.0)
+    w.params.storage = {"fp64": 0, "fp16": 2}[storage]
+    from symmetry_b200.lib import setup_workload
+    a, b = setup_workload(w), setup_workload(w)
+    a.step(30)
+    b.step(30)
+    m = a.macros()
+    a.step(20)
+    b.step(20)
+    assert np.array_equal(a.get("ri"), b.get("ri")) and np.array_equal(a.get("bi"), b.get("bi"))
+    c = setup_workload(w)
+    c.step(30)
+    m2 = c.macros()
+    c.call("calmacros")   # exports the fused state, then the reference calmacros
+    fluid = c.get("walls_all") == 0
+    for k in ("rho", "ux", "uy", "uz", "rho_N"):
+        assert np.array_equal(m[k], m2[k]), k
+        ref = c.get(k)
+        scale = max(np.abs(ref[fluid]).max(), 1e-300)
+        assert np.abs(m[k][fluid] - ref[fluid]).max() <= 1e-12 * scale, k
