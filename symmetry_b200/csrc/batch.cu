@@ -4,10 +4,9 @@
 //   k_finalize_batch  calmacros of every domain in one launch, from the colour
 //                     densities the previous collide accumulated (blocks map
 //                     to domains through a prefix sum of per-domain block counts);
-//   per-domain sparse particle coupling and pin fill (only domains with
-//                     solids; these are the small kernels of fast.cu), each
-//                     domain's chain on its own graph branch so the chains
-//                     of different domains run concurrently;
+//   sparse work       particle coupling and pin fill of every domain with
+//                     solids, one launch per subroutine for all of them
+//                     (sparse.cu);
 //   k_collide_batch   one persistent launch (one CTA per SM slot) whose CTAs
 //                     take 32x8xX tiles of any domain from a work-tile table
 //                     through an atomic counter, largest tiles first, so
@@ -138,11 +137,7 @@ struct sym_batch {
   long long nblocks = 0;
   int* d_counter = nullptr;
   int grid = 0;
-  // fork/join of the per-domain sparse chains: one branch stream per solid
-  // domain (up to kBranches, then shared round robin)
-  std::vector<cudaStream_t> branch;
-  cudaEvent_t ev_fork = nullptr;
-  std::vector<cudaEvent_t> ev_join;
+  SparsePlan* sparse = nullptr;   // particle and wall work of every domain, batched
   cudaGraph_t graph[2] = {nullptr, nullptr};
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   bool built = false;
@@ -173,6 +168,8 @@ void free_graphs(sym_batch* b) {
 }
 
 void free_tables(sym_batch* b) {
+  sparse_plan_free(b->sparse);
+  b->sparse = nullptr;
   for (int k = 0; k < 2; k++)
     if (b->d_desc[k]) { cudaFree(b->d_desc[k]); b->d_desc[k] = nullptr; }
   if (b->d_blk) { cudaFree(b->d_blk); b->d_blk = nullptr; }
@@ -206,64 +203,16 @@ DomainDesc make_desc(sym_handle* h, int cur, int pc) {
   return d;
 }
 
-constexpr int kBranches = 64;
-
-// create the branch streams and fork/join events for the solid domains
-int ensure_branches(sym_batch* b) {
-  int solid = 0;
-  for (sym_handle* h : b->doms) solid += (h->dp.par > 0 || h->dp.wall_x) ? 1 : 0;
-  const int want = std::min(solid, kBranches);
-  if (!b->ev_fork)
-    if (int e = bcuda(b, cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming), "fork event")) return e;
-  while ((int)b->branch.size() < want) {
-    cudaStream_t s = nullptr;
-    cudaEvent_t j = nullptr;
-    if (int e = bcuda(b, cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "branch stream")) return e;
-    if (int e = bcuda(b, cudaEventCreateWithFlags(&j, cudaEventDisableTiming), "join event")) {
-      cudaStreamDestroy(s);
-      return e;
-    }
-    b->branch.push_back(s);
-    b->ev_join.push_back(j);
-  }
-  return SYM_OK;
-}
-
 // One batch step on b->st (captured into a graph, or eager when timing):
 // descriptor table k, domain i at buffer parity (built_cur[i] + k) & 1.
 // ev (optional, eager only): 4 events recorded before the phase launch, after
-// it, after the sparse chains have joined, and after the collide launch.
+// it, after the sparse work, and after the collide launch.
 template <typename S>
 int enqueue_batch_step(sym_batch* b, int k, cudaEvent_t* ev) {
-  const int n = (int)b->doms.size();
   if (ev) cudaEventRecord(ev[0], b->st);
   k_finalize_batch<S><<<(unsigned)b->nblocks, 256, 0, b->st>>>(b->d_desc[k], b->d_blk);
   if (ev) cudaEventRecord(ev[1], b->st);
-  if (!b->branch.empty()) {
-    cudaEventRecord(b->ev_fork, b->st);
-    std::vector<char> used(b->branch.size(), 0);
-    int j = 0;
-    for (int i = 0; i < n; i++) {
-      sym_handle* h = b->doms[i];
-      if (!(h->dp.par > 0 || h->dp.wall_x)) continue;
-      const int q = j++ % (int)b->branch.size();
-      if (!used[q]) {
-        cudaStreamWaitEvent(b->branch[q], b->ev_fork, 0);
-        used[q] = 1;
-      }
-      const int cur = (b->built_cur[i] + k) & 1, pc = (b->built_pc[i] + k) & 1;
-      cudaStream_t saved = h->st;
-      h->st = b->branch[q];   // the domain's sparse kernels go on its branch
-      const int e = fast_enqueue_sparse(h, cur, pc);
-      h->st = saved;
-      if (e) return berr(b, e, h->err.c_str());
-    }
-    for (size_t q = 0; q < b->branch.size(); q++)
-      if (used[q]) {
-        cudaEventRecord(b->ev_join[q], b->branch[q]);
-        cudaStreamWaitEvent(b->st, b->ev_join[q], 0);
-      }
-  }
+  if (int e = sparse_enqueue(b->sparse, k, b->st)) return berr(b, e, "sparse step");
   if (ev) cudaEventRecord(ev[2], b->st);
   cudaMemsetAsync(b->d_counter + k, 0, sizeof(int), b->st);
   using R = typename Codec<S>::R;
@@ -339,7 +288,11 @@ int build(sym_batch* b) {
   if (int e = bcuda(b, cudaMalloc(&b->d_tiles, sizeof(TileEntry) * std::max(1, b->ntiles)), "tiles")) return e;
   cudaMemcpyAsync(b->d_tiles, tiles.data(), sizeof(TileEntry) * b->ntiles, cudaMemcpyHostToDevice, b->st);
   if (int e = bcuda(b, cudaStreamSynchronize(b->st), "tables")) return e;
-  if (int e = ensure_branches(b)) return e;
+  {
+    int err = SYM_OK;
+    b->sparse = sparse_plan_build(b->doms, b->built_cur, b->built_pc, b->st, &err);
+    if (!b->sparse) return berr(b, err, "sparse plan");
+  }
   for (int k = 0; k < 2; k++) {
     if (int e = bcuda(b, cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal), "capture")) return e;
     int e1 = enqueue_any(b, k, nullptr);
@@ -437,9 +390,6 @@ int sym_batch_destroy(sym_batch* b) {
   free_graphs(b);
   free_tables(b);
   if (b->d_counter) cudaFree(b->d_counter);
-  for (cudaStream_t s : b->branch) cudaStreamDestroy(s);
-  for (cudaEvent_t e : b->ev_join) cudaEventDestroy(e);
-  if (b->ev_fork) cudaEventDestroy(b->ev_fork);
   if (b->st) cudaStreamDestroy(b->st);
   delete b;
   return SYM_OK;
@@ -524,7 +474,7 @@ int sym_batch_autotune(sym_batch* b, int trial_steps, int* steps_taken) {
 }
 
 // nsteps eager (not graph) batch steps with CUDA events on the batch stream.
-// ms[0] = whole region, ms[1] = phase launches, ms[2] = per-domain sparse
+// ms[0] = whole region, ms[1] = phase launches, ms[2] = batched sparse
 // chains (fork to join), ms[3] = collide launches (sums over the steps).
 int sym_batch_step_kernels(sym_batch* b, int nsteps, double* ms) {
   if (!b || !ms || nsteps <= 0) return SYM_ERR_PARAM;

@@ -64,58 +64,13 @@ typename Acc<typename Codec<S>::R>::T* accbuf(sym_handle* h) {
   return reinterpret_cast<typename Acc<typename Codec<S>::R>::T*>(h->fast.acc);
 }
 
-int box_extent(const sym_handle* h, double margin) { return (int)std::ceil(2.0 * (h->dp.rad + margin)) + 2; }
-
-// sparse per-step work between k_finalize and k_collide: particle coupling on
-// the particle boxes and the fictitious phi on solid nodes next to fluid
-template <typename S>
-int enqueue_sparse(sym_handle* h, int cur, int pc) {
-  using R = typename Codec<S>::R;
-  const DevParams& P = h->dp;
-  const Pad pd = make_pad(P);
-  S* pin_ = popbuf<S>(h, cur);
-  R* phic = phibuf<S>(h, pc);
-  R* phip = phibuf<S>(h, 1 - pc);
-  // (L4) particle coupling on the particle boxes
-  if (P.par > 0) {
-    const double mprep = 6.0;
-    const int np = box_extent(h, mprep);
-    const long long cnt = (long long)np * np * np;
-    for (int pp = 1; pp <= P.par; pp++)
-      k_fast_prep<S><<<blocks_for(cnt), 256, 0, h->st>>>(P, pd, np, mprep, pp, h->dpart, pin_, phic, phip,
-                                                         h->walls_all, h->pout, h->rhoN, h->rhoR, h->rhoB, h->fi,
-                                                         h->gx, h->gy, h->gz, h->nx, h->ny, h->nz, rr_old(h, pc));
-    int e;
-    if ((e = part_lagrange_points(h))) return e;
-    if ((e = part_capillary_force2(h))) return e;
-    if ((e = part_momentum(h))) return e;
-    if ((e = part_repulsive(h))) return e;
-    if ((e = part_movement(h))) return e;
-    if ((e = part_set_walls(h))) return e;
-    if ((e = part_refilling(h))) return e;
-    const double mref = 4.0;
-    const int nr = box_extent(h, mref);
-    const long long cr = (long long)nr * nr * nr;
-    for (int pp = 1; pp <= P.par; pp++)
-      k_fast_refill_import<S><<<blocks_for(cr), 256, 0, h->st>>>(P, pd, nr, mref, pp, h->dpart, pin_, phic, h->pout,
-                                                                   h->walls_old, h->ri, h->bi, h->rhoN,
-                                                                   rr_old(h, pc));
-  }
-  // (a2) fictitious phi on solid nodes next to fluid
-  if (P.wall_x) {
-    const unsigned g = blocks_for((long long)P.ny * P.nz);
-    k_fast_pinfill_plane<R><<<g, 256, 0, h->st>>>(P, pd, phic, h->pin, h->walls_all, 0);
-    k_fast_pinfill_plane<R><<<g, 256, 0, h->st>>>(P, pd, phic, h->pin, h->walls_all, P.nx - 1);
-  }
-  if (P.par > 0) {
-    const double mpin = 2.0;
-    const int np = box_extent(h, mpin);
-    const long long cnt = (long long)np * np * np;
-    for (int pp = 1; pp <= P.par; pp++)
-      k_fast_pinfill_box<R><<<blocks_for(cnt), 256, 0, h->st>>>(P, pd, np, mpin, pp, h->dpart, phic, h->pin,
-                                                                h->walls_all);
-  }
-  return check_cuda(h, cudaGetLastError(), "fast sparse step");
+// the particle and wall work of this handle's fused steps (sparse.cu); built
+// outside any stream capture
+int ensure_sparse(sym_handle* h) {
+  if (h->fast.sparse || !has_solids(h)) return SYM_OK;
+  int err = SYM_OK;
+  h->fast.sparse = sparse_plan_build({h}, {0}, {0}, h->st, &err);
+  return h->fast.sparse ? SYM_OK : set_error(h, err, "sparse plan");
 }
 
 // ev (optional): 4 events recorded before k_finalize, after it, before
@@ -139,7 +94,8 @@ int enqueue_step(sym_handle* h, int cur, int pc, cudaEvent_t* ev) {
     k_finalize<S, false><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, accbuf<S>(h), phic, h->walls_all, rr_new(h, pc),
                                                              h->fast.status);
   if (ev) cudaEventRecord(ev[1], h->st);
-  if (int e = enqueue_sparse<S>(h, cur, pc)) return e;
+  // particle coupling and pin fill (cur and pc advance together from 0)
+  if (int e = sparse_enqueue(h->fast.sparse, cur, h->st)) return set_error(h, e, "sparse step");
   // (a3-a9) fused derivatives + collision + recolour + stream + bounce-back
   const int xc = h->fast.xchunk > 0 ? h->fast.xchunk : XCHUNK;
   dim3 grid((P.nz + BZ - 1) / BZ, (P.ny + BY - 1) / BY, (P.nx + xc - 1) / xc);
@@ -191,14 +147,6 @@ __global__ void __launch_bounds__(256) k_neck_planes(DevParams P, Pad pd, const 
     __syncthreads();
   }
   if (threadIdx.x == 0) out[z] = sh[0];
-}
-
-int enqueue_sparse_any(sym_handle* h, int cur, int pc) {
-  switch (h->fast.storage) {
-    case SYM_STORE_FP64: return enqueue_sparse<double>(h, cur, pc);
-    case SYM_STORE_FP32: return enqueue_sparse<float>(h, cur, pc);
-    default: return enqueue_sparse<__half>(h, cur, pc);
-  }
 }
 
 int enqueue(sym_handle* h, int cur, int pc, cudaEvent_t* ev = nullptr) {
@@ -256,6 +204,8 @@ int fast_alloc(sym_handle* h) {
 
 void fast_free(sym_handle* h) {
   FastState& F = h->fast;
+  sparse_plan_free(F.sparse);
+  F.sparse = nullptr;
   for (int k = 0; k < 2; k++) {
     dev_release(h, F.pop[k]);
     dev_release(h, F.phi[k]);
@@ -354,6 +304,7 @@ int fast_macros(sym_handle* h) {
 // its own captured graph
 int fast_step(sym_handle* h, int nsteps) {
   FastState& F = h->fast;
+  if (int e = ensure_sparse(h)) return e;
   for (int t = 0; t < nsteps; t++) {
     const int k = F.cur;   // cur and pc advance together
     if (!F.gexec[k]) {
@@ -377,10 +328,10 @@ int fast_step(sym_handle* h, int nsteps) {
 // nsteps eager (not graph) steps with CUDA events around the kernel classes.
 // ms[0] = whole region, ms[1] = sum of k_finalize, ms[2] = sum of the sparse
 // particle/pin-fill work, ms[3] = sum of k_collide.
-int fast_enqueue_sparse(sym_handle* h, int cur, int pc) { return enqueue_sparse_any(h, cur, pc); }
 
 int fast_step_timed(sym_handle* h, int nsteps, double ms[4]) {
   FastState& F = h->fast;
+  if (int e = ensure_sparse(h)) return e;
   std::vector<cudaEvent_t> ev(4 * (size_t)nsteps + 2);
   for (auto& e : ev)
     if (int r = check_cuda(h, cudaEventCreate(&e), "event")) return r;

@@ -638,13 +638,15 @@ __global__ void __launch_bounds__(TPB, collide_ctas<S>()) k_collide(DevParams P,
                          &tm_phi, &tm_rinv, blockIdx.x * BZ, blockIdx.y * BY, xa, min(xa + xchunk, P.nx), sm, nload);
 }
 
-// ---- pin fill on the fused state (derivatives :467-492) ----------------------------
+// ---- the fused state's side of the particle and wall work ---------------------------
+// (device bodies; the batched launches are in sparse.cu)
+
+// pin fill (derivatives :467-492): fictitious phi of solid node (x,y,z) next
+// to fluid = wi-weighted mean of its fluid neighbours
 template <typename R>
-__global__ void k_fast_pinfill_plane(DevParams P, Pad pd, R* phi, const int32_t* __restrict__ pin,
-                                     const int32_t* __restrict__ walls_all, int xplane) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= P.ny * P.nz) return;
-  const int y = t / P.nz, z = t % P.nz, x = xplane;
+__device__ __forceinline__ void pinfill_node(const DevParams& P, const Pad& pd, R* phi,
+                                             const int32_t* __restrict__ pin, const int32_t* __restrict__ walls_all,
+                                             int x, int y, int z) {
   const long long L = lin(P, x, y, z);
   if (pin[L] <= 0) return;
   R ws = R(0), v = R(0);
@@ -656,62 +658,20 @@ __global__ void k_fast_pinfill_plane(DevParams P, Pad pd, R* phi, const int32_t*
   phi_store<R>(P, pd, phi, x, y, z, v / ws);
 }
 
-// node of a particle box (origin from the device-resident centre; see particles.cu)
-__device__ __forceinline__ bool fbox_node(const DevParams& P, int n, double margin, const double* centre, int pp,
-                                          long long t, int& x, int& y, int& z) {
-  if (t >= (long long)n * n * n) return false;
-  int id[3];
-  id[2] = (int)(t % n);
-  t /= n;
-  id[1] = (int)(t % n);
-  id[0] = (int)(t / n);
-  const int dims[3] = {P.nx, P.ny, P.nz};
-  int v[3];
-  for (int k = 0; k < 3; k++) {
-    const double c = centre[k * P.par + pp - 1] - (double)P.origin;
-    int q = (int)floor(c - P.rad - margin) + id[k];
-    const bool periodic = !(k == 0 && P.wall_x);
-    if (n >= dims[k]) q = id[k];
-    if (q >= dims[k] && n >= dims[k]) return false;
-    if (periodic) q = ((q % dims[k]) + dims[k]) % dims[k];
-    else if (q < 0 || q >= dims[k]) return false;
-    v[k] = q;
-  }
-  x = v[0]; y = v[1]; z = v[2];
-  return true;
-}
-
-template <typename R>
-__global__ void k_fast_pinfill_box(DevParams P, Pad pd, int n, double margin, int pp,
-                                   const sym_particles* __restrict__ Sp, R* phi, const int32_t* __restrict__ pin,
-                                   const int32_t* __restrict__ walls_all) {
-  int x, y, z;
-  if (!fbox_node(P, n, margin, Sp->center, pp, blockIdx.x * (long long)blockDim.x + threadIdx.x, x, y, z)) return;
-  const long long L = lin(P, x, y, z);
-  if (pin[L] <= 0) return;
-  R ws = R(0), v = R(0);
-#pragma unroll
-  for (int i = 1; i < 19; i++) {
-    const long long nb = lin(P, wrapi(x + CX(i), P.nx), wrapi(y + CY(i), P.ny), wrapi(z + CZ(i), P.nz));
-    if (walls_all[nb] <= 0) { ws = ws + R(W(i)); v = v + R(W(i)) * phi[pd.idx(x + CX(i), y + CY(i), z + CZ(i))]; }
-  }
-  phi_store<R>(P, pd, phi, x, y, z, v / ws);
-}
-
-// ---- particle preparation: canonical views of the fused state on a particle box ----
-// rho_N (this step's calmacros), rho_R/rho_B and fi (current populations), and the
-// previous step's gradient/normal (from the previous pin-filled phi) -- what
-// Lagrange_points, momentum and refilling read.
+// particle preparation: canonical views of the fused state at a node of a
+// particle box -- rho_N (this step's calmacros), rho_R/rho_B and fi (current
+// populations), and the previous step's gradient/normal (from the previous
+// pin-filled phi): what Lagrange_points, momentum and refilling read.
+// rr_old (16-bit storage): 1/rho_ref of the populations.
 template <typename S>
-__global__ void k_fast_prep(DevParams P, Pad pd, int n, double margin, int pp, const sym_particles* __restrict__ Sp,
-                            const S* __restrict__ pops, const typename Codec<S>::R* __restrict__ phi_cur,
-                            const typename Codec<S>::R* __restrict__ phi_prev,
-                            const int32_t* __restrict__ walls_all, const int32_t* __restrict__ pout,
-                            double* rhoN, double* rhoR, double* rhoB, double* fi, double* gx, double* gy,
-                            double* gz, double* nxv, double* nyv, double* nzv, const float* __restrict__ rr_old) {
+__device__ __forceinline__ void prep_node(const DevParams& P, const Pad& pd, const sym_particles* __restrict__ Sp,
+                                          const S* __restrict__ pops, const typename Codec<S>::R* __restrict__ phi_cur,
+                                          const typename Codec<S>::R* __restrict__ phi_prev,
+                                          const int32_t* __restrict__ walls_all, const int32_t* __restrict__ pout,
+                                          double* rhoN, double* rhoR, double* rhoB, double* fi, double* gx,
+                                          double* gy, double* gz, double* nxv, double* nyv, double* nzv,
+                                          const float* __restrict__ rr_old, int x, int y, int z) {
   using R = typename Codec<S>::R;
-  int x, y, z;
-  if (!fbox_node(P, n, margin, Sp->center, pp, blockIdx.x * (long long)blockDim.x + threadIdx.x, x, y, z)) return;
   const long long L = lin(P, x, y, z);
   const unsigned N = (unsigned)P.N;
   const R rref = Codec<S>::kRef ? R(1) / R(rr_old[pd.idx(x, y, z)]) : R(P.rho0);
@@ -753,22 +713,19 @@ __global__ void k_fast_prep(DevParams P, Pad pd, int n, double margin, int pp, c
   gx[L] = g0; gy[L] = g1; gz[L] = g2; nxv[L] = n0; nyv[L] = n1; nzv[L] = n2;
 }
 
-// after refilling: refilled nodes' canonical populations and phi into the fused state
+// after refilling: a refilled node's canonical populations and phi into the
+// fused state (encoded with the reference this step's collide decodes with)
 template <typename S>
-__global__ void k_fast_refill_import(DevParams P, Pad pd, int n, double margin, int pp,
-                                     const sym_particles* __restrict__ Sp, S* pops,
-                                     typename Codec<S>::R* phi_cur, const int32_t* __restrict__ pout,
-                                     const int32_t* __restrict__ walls_old, const double* __restrict__ ri,
-                                     const double* __restrict__ bi, const double* __restrict__ rhoN,
-                                     const float* __restrict__ rr_old) {
+__device__ __forceinline__ void refill_import_node(const DevParams& P, const Pad& pd, int pp, S* pops,
+                                                   typename Codec<S>::R* phi_cur, const int32_t* __restrict__ pout,
+                                                   const int32_t* __restrict__ walls_old,
+                                                   const double* __restrict__ ri, const double* __restrict__ bi,
+                                                   const double* __restrict__ rhoN, const float* __restrict__ rr_old,
+                                                   int x, int y, int z) {
   using R = typename Codec<S>::R;
-  int x, y, z;
-  if (!fbox_node(P, n, margin, Sp->center_old, pp, blockIdx.x * (long long)blockDim.x + threadIdx.x, x, y, z))
-    return;
   const long long L = lin(P, x, y, z);
   const unsigned N = (unsigned)P.N;
   if (pout[L] != pp || walls_old[L] < 1) return;
-  // the collide of this step decodes these populations with rr_old
   const R irr = Codec<S>::kRef ? R(rr_old[pd.idx(x, y, z)]) : R(1.0 / P.rho0);
   unroll19([&](auto ic) {
     constexpr int i = decltype(ic)::value;

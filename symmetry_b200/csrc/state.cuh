@@ -3,10 +3,13 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <string>
+#include <vector>
 #include "../../include/symmetry.h"
 #include "lattice.cuh"
 
 namespace symb200 {
+
+struct SparsePlan;   // sparse.cu
 
 // Fused fast-path state (CONFIG mode).  Populations are stored post-stream
 // (push streaming), structure of arrays [colour][velocity][node], in the
@@ -27,6 +30,7 @@ struct FastState {
   CUtensorMap tm_phi[2] = {};
   CUtensorMap tm_rinv[2] = {};
   bool valid = false;      // fast state holds the authoritative populations
+  SparsePlan* sparse = nullptr;   // particle and wall work of sym_step (built on first use)
   size_t bytes = 0;
   cudaGraph_t graph[2] = {nullptr, nullptr};       // one captured step per buffer parity
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
@@ -115,8 +119,16 @@ int fast_export(sym_handle* h);   // fast -> canonical
 int fast_macros(sym_handle* h);   // calmacros of the fused populations into rho, u, rho_N (fused state kept)
 int fast_step(sym_handle* h, int nsteps);
 int fast_step_timed(sym_handle* h, int nsteps, double ms[4]);
-int fast_enqueue_sparse(sym_handle* h, int cur, int pc);   // particles + pin fill on h->st
 int fast_neck_planes(sym_handle* h, double* out, cudaStream_t st);   // per-z red area, nz doubles
+
+// particle and wall work of fused steps, batched (sparse.cu): the plan for
+// `doms` at buffer parities cur0/pc0 for step parity 0, its launches for step
+// parity k, launches per step
+SparsePlan* sparse_plan_build(const std::vector<sym_handle*>& doms, const std::vector<int>& cur0,
+                              const std::vector<int>& pc0, cudaStream_t st, int* err);
+int sparse_enqueue(SparsePlan* p, int k, cudaStream_t st);
+int sparse_launches(const SparsePlan* p);
+void sparse_plan_free(SparsePlan* p);
 
 // batch engine, batch.cu
 int batch_launch(sym_batch* b, int nsteps);   // enqueue nsteps graph steps, no synchronisation
