@@ -94,14 +94,12 @@ __global__ void __launch_bounds__(kTPB, collide_ctas<S>()) k_collide_batch(const
     __syncthreads();
     const DomainDesc& D = s_desc;
     using AT = typename Acc<R>::T;
-    if (D.solid)
-      collide_tile<S, true>(D.P, D.pd, (const S*)D.pin, (S*)D.pnext, (const R*)D.phic, D.walls, D.walls_all, D.pout,
-                            D.Sp, D.ffi, D.rr_old, D.rr_new, (AT*)D.acc, D.status, D.tm_phi, D.tm_rinv, e.z0,
-                            e.y0, e.xa, e.xb, sm, nload);
-    else
-      collide_tile<S, false>(D.P, D.pd, (const S*)D.pin, (S*)D.pnext, (const R*)D.phic, D.walls, D.walls_all,
-                             D.pout, D.Sp, D.ffi, D.rr_old, D.rr_new, (AT*)D.acc, D.status, D.tm_phi, D.tm_rinv,
-                             e.z0, e.y0, e.xa, e.xb, sm, nload);
+    // one compiled variant for every tile (solid handling switched per
+    // domain): the instruction working set of the persistent kernel stays
+    // that of one variant
+    collide_tile<S, true>(D.P, D.pd, (const S*)D.pin, (S*)D.pnext, (const R*)D.phic, D.walls, D.walls_all, D.pout,
+                          D.Sp, D.ffi, D.rr_old, D.rr_new, (AT*)D.acc, D.status, D.tm_phi, D.tm_rinv, e.z0, e.y0,
+                          e.xa, e.xb, sm, nload, D.solid != 0);
     __syncthreads();
   }
 }
@@ -475,7 +473,7 @@ int sym_batch_autotune(sym_batch* b, int trial_steps, int* steps_taken) {
 
 // nsteps eager (not graph) batch steps with CUDA events on the batch stream.
 // ms[0] = whole region, ms[1] = phase launches, ms[2] = batched sparse
-// chains (fork to join), ms[3] = collide launches (sums over the steps).
+// work, ms[3] = collide launches (sums over the steps).
 int sym_batch_step_kernels(sym_batch* b, int nsteps, double* ms) {
   if (!b || !ms || nsteps <= 0) return SYM_ERR_PARAM;
   cudaSetDevice(b->device);

@@ -74,6 +74,7 @@ void fill_devparams(const sym_params& p, DevParams& d) {
   d.rho0 = p.rho0; d.nu_r = p.nu_r; d.nu_b = p.nu_b;
   d.s_e = p.s_e; d.s_eps = p.s_eps; d.s_q = p.s_q; d.s_pi = p.s_pi; d.s_m = p.s_m;
   d.sigma = p.sigma; d.beta = p.beta; d.cita = p.cita;
+  d.sin_cita = std::sin(p.cita); d.cos_cita = std::cos(p.cita);
   for (int k = 0; k < 3; k++) d.body[k] = p.body[k];
   d.rad = p.rad;
   d.mass = p.mass > 0 ? p.mass : 4.0 / 3.0 * p.rho_p * M_PI * (p.rad * p.rad * p.rad);

@@ -198,7 +198,7 @@ __device__ __forceinline__ void finalize_node(const DevParams& P, const Pad& pd,
   R rho = R(P.rho0);
   if (!(SOLID && walls_all[L] >= 1)) {
     rho = sr + sb;
-    v = (sr - sb) / rho;
+    v = qdiv<R>(sr - sb, rho);
   }
   if (*status) v = R(NAN);
   phi_store<R>(P, pd, phi, x, y, z, v);
@@ -222,7 +222,7 @@ __device__ __forceinline__ void wet_rotate(const DevParams& P, const sym_particl
   const R nw[3] = {R(nwd[0]), R(nwd[1]), R(nwd[2])};
   const R n[3] = {n0, n1, n2};
   R v[3];
-  akai_rotate<R>(R(P.cita), nw, n, true, v);
+  akai_rotate_sc<R>(R(P.sin_cita), R(P.cos_cita), nw, n, true, v);
   n0 = v[0]; n1 = v[1]; n2 = v[2];
 }
 
@@ -294,8 +294,12 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
                                              const float* __restrict__ rr_old, const float* __restrict__ rr_new,
                                              typename Acc<typename Codec<S>::R>::T* acc, int* status,
                                              const CUtensorMap* tm_phi, const CUtensorMap* tm_rinv,
-                                             int z0, int y0, int xa, int xb, Smem<S>& sm, unsigned& nload) {
+                                             int z0, int y0, int xa, int xb, Smem<S>& sm, unsigned& nload,
+                                             bool solid_rt = true) {
   using R = typename Codec<S>::R;
+  // solid handling: compiled in (SOLID) and wanted by this domain (solid_rt);
+  // the batched kernel compiles one variant and decides per tile
+  const bool SOLIDX = SOLID && solid_rt;
   constexpr bool REF = Codec<S>::kRef;
   const int tz = threadIdx.x % BZ, ty = threadIdx.x / BZ;
   const unsigned N = (unsigned)P.N;
@@ -332,7 +336,7 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
       R n0 = R(0), n1 = R(0), n2 = R(0), fn = R(0);
       bool ok = y <= P.ny && z <= P.nz;
       int pp = 0;
-      if (SOLID && ok) {
+      if (SOLIDX && ok) {
         const unsigned Lw = (unsigned)(wrapi(z, P.nz) + sy * wrapi(y, P.ny) + sx * wrapi(xp, P.nx));
         if (walls_all[Lw] > 0) ok = false;
         else pp = pout[Lw];
@@ -351,9 +355,9 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
         g0 = R(3) * g0; g1 = R(3) * g1; g2 = R(3) * g2;
         fn = sqrt(g0 * g0 + g1 * g1 + g2 * g2);
         if (fn > evap) {
-          const R rf = R(1) / fn;
+          const R rf = qdiv<R>(R(1), fn);
           n0 = g0 * rf; n1 = g1 * rf; n2 = g2 * rf;
-          if (SOLID && pp >= 1) wet_rotate<R>(P, Sp, pp, wrapi(xp, P.nx), wrapi(y, P.ny), wrapi(z, P.nz), n0, n1, n2);
+          if (SOLIDX && pp >= 1) wet_rotate<R>(P, Sp, pp, wrapi(xp, P.nx), wrapi(y, P.ny), wrapi(z, P.nz), n0, n1, n2);
         } else {
           fn = R(0);
         }
@@ -399,7 +403,7 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
     const unsigned L = (unsigned)(zc + sy * yc + sx * x);
     int pp = 0;
     bool act = inr;
-    if (SOLID) {
+    if (SOLIDX) {
       if (walls_all[L] > 0) act = false;
       else pp = pout[L];
     }
@@ -440,7 +444,7 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
       if (CY(i)) uy = uy + f[i] * R(CY(i));
       if (CZ(i)) uz = uz + f[i] * R(CZ(i));
     }
-    const R irho = R(1) / rho;
+    const R irho = qdiv<R>(R(1), rho);
     ux = ux * irho; uy = uy * irho; uz = uz * irho;
     const int s1 = x % 4;
     const NormalV<R> nown = sm.n[s1][ty + 1][tz + 1];
@@ -449,7 +453,7 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
     const R rhoN = PHI(x, ty + 2, tz + 2);
     // CSF surface tension from the curvature of the normal field (:624-667)
     R fx = R(0), fy = R(0), fz = R(0);
-    if (flag && (!SOLID || pp <= 0)) {
+    if (flag && (!SOLIDX || pp <= 0)) {
       // d_ba = sum_i w_i c_ia n_b(x + c_i) (:635-660), over the nine opposite
       // pairs: w_i c_ia (n_b(x + c_i) - n_b(x - c_i))
       R d00 = 0, d01 = 0, d02 = 0, d10 = 0, d11 = 0, d12 = 0, d20 = 0, d21 = 0, d22 = 0;
@@ -480,7 +484,7 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
     // post-collision populations for the momentum exchange (:1241-1243), read
     // only next to particles (pout = particle id); wall planes (ids > par)
     // need none, and a handle without particles holds no ffi array
-    if (SOLID && act && pp >= 1 && pp <= P.par) {
+    if (SOLIDX && act && pp >= 1 && pp <= P.par) {
 #pragma unroll
       for (int i = 0; i < 19; i++) ffi[(size_t)i * N + L] = (double)f[i];
     }
@@ -492,6 +496,18 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
     const R ratio = bzero ? R(1) : (rzero ? R(0) : sr * irho);
     const R coef = (bzero || rzero || !flag) ? R(0) : sr * sb * irho * R(P.beta);
     const bool exp_ = x == xb - 1, exm = x == xa;
+    // rigid-body velocity of particle pp at this node (curve :1009-1014), for
+    // the links that bounce back from it
+    R uw0 = R(0), uw1 = R(0), uw2 = R(0);
+    if (SOLIDX && pp >= 1 && pp <= P.par) {
+      const int par = P.par;
+      const R xr = R(disp(P, (double)(x + P.origin), Sp->center[0 * par + pp - 1], 0));
+      const R yr = R(disp(P, (double)(y + P.origin), Sp->center[1 * par + pp - 1], 1));
+      const R zr = R(disp(P, (double)(z + P.origin), Sp->center[2 * par + pp - 1], 2));
+      uw0 = R(Sp->up[0 * par + pp - 1]) + zr * R(Sp->rp[1 * par + pp - 1]) - yr * R(Sp->rp[2 * par + pp - 1]);
+      uw1 = R(Sp->up[1 * par + pp - 1]) + xr * R(Sp->rp[2 * par + pp - 1]) - zr * R(Sp->rp[0 * par + pp - 1]);
+      uw2 = R(Sp->up[2 * par + pp - 1]) + yr * R(Sp->rp[0 * par + pp - 1]) - xr * R(Sp->rp[1 * par + pp - 1]);
+    }
     // neighbour offsets with the periodic wrap folded in (one select per face)
     const int oxp = (x == P.nx - 1) ? -(P.nx - 1) * sx : sx, oxm = (x == 0) ? (P.nx - 1) * sx : -sx;
     const int oyp = (yc == P.ny - 1) ? -(P.ny - 1) * sy : sy, oym = (yc == 0) ? (P.ny - 1) * sy : -sy;
@@ -509,26 +525,13 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
         const unsigned T = L + (CX(i) > 0 ? oxp : (CX(i) < 0 ? oxm : 0)) +
                            (CY(i) > 0 ? oyp : (CY(i) < 0 ? oym : 0)) + (CZ(i) > 0 ? ozp : (CZ(i) < 0 ? ozm : 0));
         if (!act) return;
-        if (SOLID && i > 0 && pp >= 1) {
+        if (SOLIDX && i > 0 && pp >= 1) {
           const int wb = walls[T];
           const bool flat = wb > P.par;
           if (wb == pp || flat) {
             // curve (:1001-1019): link OPC(i) of this node comes back reversed
             constexpr int j = OPC(i);
-            R star = R(0);
-            if (!flat) {
-              const int par = P.par;
-              const R xr = R(disp(P, (double)(x + P.origin), Sp->center[0 * par + wb - 1], 0));
-              const R yr = R(disp(P, (double)(y + P.origin), Sp->center[1 * par + wb - 1], 1));
-              const R zr = R(disp(P, (double)(z + P.origin), Sp->center[2 * par + wb - 1], 2));
-              const R uw0 = R(Sp->up[0 * par + wb - 1]) + zr * R(Sp->rp[1 * par + wb - 1]) -
-                            yr * R(Sp->rp[2 * par + wb - 1]);
-              const R uw1 = R(Sp->up[1 * par + wb - 1]) + xr * R(Sp->rp[2 * par + wb - 1]) -
-                            zr * R(Sp->rp[0 * par + wb - 1]);
-              const R uw2 = R(Sp->up[2 * par + wb - 1]) + yr * R(Sp->rp[0 * par + wb - 1]) -
-                            xr * R(Sp->rp[1 * par + wb - 1]);
-              star = uw0 * R(CX(j)) + uw1 * R(CY(j)) + uw2 * R(CZ(j));
-            }
+            const R star = flat ? R(0) : uw0 * R(CX(j)) + uw1 * R(CY(j)) + uw2 * R(CZ(j));
             const R rr = r + R(6.0 * W(j)) * sr * star;
             const R bb = (f[i] - r) + R(6.0 * W(j)) * sb * star;
             const R irr = REF ? R(sm.irr[x % kIrrRing][(ty + 2) * (BZ + 4) + tz + 2]) : irho0;

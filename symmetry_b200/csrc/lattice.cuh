@@ -94,11 +94,20 @@ struct DevParams {
   double sigma, beta, cita;
   double body[3];
   double rad, mass, inertia, fg, alpha, evap;
+  double sin_cita, cos_cita;   // of the contact angle (fused path)
   double inu_r, inu_b;     // 1/nu_r, 1/nu_b (fused path)
 };
 
 template <typename T>
 __device__ __forceinline__ T wrapi(T v, T n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
+
+// a / b: IEEE division in FP64; in FP32 arithmetic (the FP32 and 16-bit
+// storage paths) the fast reciprocal-based quotient (2 ulp), whose error is far
+// below the storage rounding
+template <typename R>
+__device__ __forceinline__ R qdiv(R a, R b) { return a / b; }
+template <>
+__device__ __forceinline__ float qdiv<float>(float a, float b) { return __fdividef(a, b); }
 
 __device__ __forceinline__ long long lin(const DevParams& P, int x, int y, int z) {
   return (long long)z + (long long)P.nz * ((long long)y + (long long)P.ny * (long long)x);
@@ -196,8 +205,8 @@ __device__ __forceinline__ void node_rates_fast(const DevParams& P, R rhoN, R& s
                                                 R& sm) {
   const R ph = fmin(fmax(rhoN, R(-1)), R(1));
   const R D = (R(1) + ph) * R(P.inu_r) + (R(1) - ph) * R(P.inu_b);
-  su = R(2) * D / (R(12) + D);
-  const R sq_ = R(8) * (R(2) - su) / (R(8) - su);
+  su = qdiv<R>(R(2) * D, R(12) + D);
+  const R sq_ = qdiv<R>(R(8) * (R(2) - su), R(8) - su);
   se = P.s_e > 0 ? R(P.s_e) : su;
   seps = P.s_eps > 0 ? R(P.s_eps) : su;
   sq = P.s_q > 0 ? R(P.s_q) : sq_;
@@ -355,7 +364,14 @@ __device__ __forceinline__ void veccross(const double a[3], const double b[3], d
 // for angles up to ~3.5e-4, where the acos form divides by sin(0) = 0.
 // FP64 keeps the reference's expressions unchanged.
 template <typename R>
+__device__ __forceinline__ void akai_rotate_sc(R sc, R cc, const R nw[3], const R n[3], bool guard, R out[3]);
+template <typename R>
 __device__ __forceinline__ void akai_rotate(R cita, const R nw[3], const R n[3], bool guard, R out[3]) {
+  akai_rotate_sc<R>(sin(cita), cos(cita), nw, n, guard, out);
+}
+// the same with sin(cita) and cos(cita) given
+template <typename R>
+__device__ __forceinline__ void akai_rotate_sc(R sc, R cc, const R nw[3], const R n[3], bool guard, R out[3]) {
   const R mx = fmax(fabs(nw[0] - n[0]), fmax(fabs(nw[1] - n[1]), fabs(nw[2] - n[2])));
   R ct, st;
   if (sizeof(R) == 4) {
@@ -374,7 +390,6 @@ __device__ __forceinline__ void akai_rotate(R cita, const R nw[3], const R n[3],
     ct = cos(theta);
     st = sin(theta);
   }
-  const R sc = sin(cita), cc = cos(cita);
   const R a1 = cc - sc * ct / st;
   const R a2 = cc + sc * ct / st;
   const R b1 = sc / st;
