@@ -163,6 +163,16 @@ int sym_get_particles(sym_handle* h, sym_particles* s);
 int sym_get_lagrange(sym_handle* h, double* lax, double* lay, double* laz, double* la_rhon,
                      double* la_nx, double* la_ny, double* la_nz, int32_t* la_flag, double* ds);
 
+/* ---- checkpoint / restart --------------------------------------------------
+ * No counterpart in the reference, whose OUT_t.dat files hold macroscopic
+ * fields only (Source1.f90:898-924) and cannot restart a run.  save writes the
+ * handle's complete stepping state to `path`; load restores it into a handle
+ * created with the same sym_params, after which stepping continues bit for
+ * bit as if the run had not stopped.  The fused state of a sym_step handle is
+ * saved in its storage format (no re-encoding). */
+int sym_checkpoint_save(sym_handle* h, const char* path);
+int sym_checkpoint_load(sym_handle* h, const char* path);
+
 /* ---- initial state --------------------------------------------------------
  * sym_initia_center     <- initia_center   Source1.f90:926-976 (REFERENCE only)
  * sym_initialization    <- initialization  Source1.f90:850-896 (REFERENCE only)

@@ -59,6 +59,8 @@ def lib() -> ctypes.CDLL:
         L.sym_get_field.argtypes = [H, ctypes.c_int, ctypes.c_void_p]
         L.sym_set_populations.argtypes = [H, ctypes.c_void_p, ctypes.c_void_p]
         L.sym_get_macros.argtypes = [H] + [ctypes.c_void_p] * 5
+        L.sym_checkpoint_save.argtypes = [H, ctypes.c_char_p]
+        L.sym_checkpoint_load.argtypes = [H, ctypes.c_char_p]
         L.sym_set_particles.argtypes = [H, ctypes.POINTER(SymParticles)]
         L.sym_get_particles.argtypes = [H, ctypes.POINTER(SymParticles)]
         L.sym_get_lagrange.argtypes = [H] + [ctypes.c_void_p] * 9
@@ -174,6 +176,14 @@ class Lattice:
                 raise ValueError(f"{k}: contiguous float64 array of {self.p.n_nodes} values expected")
         self._ck(lib().sym_get_macros(self.h, *(out[k].ctypes.data for k in names)), "get_macros")
         return out
+
+    def save(self, path: str):
+        """Checkpoint the complete stepping state to `path`."""
+        self._ck(lib().sym_checkpoint_save(self.h, os.fsencode(path)), "checkpoint save")
+
+    def load(self, path: str):
+        """Restore a checkpoint written by a handle with the same parameters."""
+        self._ck(lib().sym_checkpoint_load(self.h, os.fsencode(path)), "checkpoint load")
 
     def set_populations(self, ri: np.ndarray, bi: np.ndarray):
         """Both colours from host arrays (pinned memory gives full PCIe rate)."""
