@@ -326,6 +326,32 @@ int sym_output3(sym_handle* h, double* hmin, int32_t* y0);
 int sym_neck_radius(sym_handle* h, double* rmin);
 /* FP64 sums over fluid nodes: out[0]=sum rho_R, [1]=sum rho_B, [2..4]=momentum. */
 int sym_mass_momentum(sym_handle* h, double out[5]);
+/* The energy budget of output4 (Source1.f90:1719-1797) before normalisation,
+ * from calmacros of the current populations (the stepping state is kept):
+ * out[0] pressure energy sum (rho-rho0)/3 and out[1] kinetic energy
+ * sum rho|u|^2/2 over red fluid nodes, out[2] interface nodes (fluid nodes with
+ * a fluid neighbour of the other colour), out[3] particle kinetic energy,
+ * out[4] capillary power (tension.up + tension_t.rp), out[5] immersed area
+ * sum Shb; particles that start on a mirror plane count half (:1765-1779).
+ * The reference's walls_all(z,y,z), rho(z,y,z) and uz(z,y,z) (:1736, :1739)
+ * read (z,y,x) here. */
+int sym_energy(sym_handle* h, double out[6]);
+/* Writers of the reference's output step (Source1.f90:218-234), Tecplot
+ * ASCII with its variables and formats.  The logs get one record per call
+ * appended (the header and a new file at t = 0; the reference re-opens them
+ * on each call and keeps only the last record):
+ *   sym_output_results  OUT file of output_results (:898-924): x,y,z (1-based),
+ *                       walls_all, rho_N, u, v, w, rho of calmacros
+ *   sym_output_result2  prefix + "P_<pp>.dat" of output_result2 (:1420-1441)
+ *   sym_output3_write   the neck record of output3 (:1673-1717): t, t/tr,
+ *                       hmin/rad_c, y0/lamda_d
+ *   sym_output4         the Energy.dat record of output4 (:1751-1792): energies
+ *                       over pi rad_c^2 sigma (times 8 in REFERENCE mode, the
+ *                       reference's 1/8 domain); *wcap_acc carries Wcap_old */
+int sym_output_results(sym_handle* h, const char* path);
+int sym_output_result2(sym_handle* h, const char* prefix, int t, double tr);
+int sym_output3_write(sym_handle* h, const char* path, int t, double tr, double rad_c, double lamda_d);
+int sym_output4(sym_handle* h, const char* path, int t, double tr, double rad_c, double* wcap_acc);
 
 /* The same five sums for callers that may not allocate device memory: no
  * counterpart in the reference.  It is meant for code that never creates a

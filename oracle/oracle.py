@@ -53,6 +53,7 @@ def lib():
                                   ctypes.POINTER(ctypes.c_int32)]
         L.orc_neck_radius.restype = ctypes.c_double
         L.orc_neck_radius.argtypes = [ctypes.c_void_p]
+        L.orc_energy.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.orc_threads.restype = ctypes.c_int
         _lib = L
     return _lib
@@ -121,6 +122,12 @@ class Oracle:
 
     def neck_radius(self) -> float:
         return lib().orc_neck_radius(self.h)
+
+    def energy(self) -> np.ndarray:
+        """output4's field sums on the arrays of the last calmacros."""
+        out = np.zeros(3)
+        lib().orc_energy(self.h, out.ctypes.data)
+        return out
 
 
 def threads() -> int:

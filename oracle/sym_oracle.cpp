@@ -1204,6 +1204,40 @@ void orc_output3(void* h, double* hmin_out, int32_t* y0_out) {
   *y0_out = y0;
 }
 
+// output4 field sums (Source1.f90:1729-1750) on the arrays of the last
+// calmacros: out[0] = sum (rho - rho0)/3 and out[1] = sum rho |u|^2 / 2 over
+// red fluid nodes, out[2] = fluid nodes with a fluid neighbour of the other
+// colour.  The reference's walls_all(z,y,z), rho(z,y,z), uz(z,y,z) (:1736,
+// :1739) are read at (z,y,x).  REFERENCE: x,y,z in 2..n-1 (:1730-1732);
+// CONFIG: every node with periodic neighbours.
+void orc_energy(void* h, double* out) {
+  Orc& o = *(Orc*)h;
+  double epv = 0.0, emov = 0.0, area = 0.0;
+  const int lo = o.ref ? 2 : 1, dx = o.ref ? 1 : 0;
+  for (int x = lo; x <= o.nx - dx; x++)
+    for (int y = lo; y <= o.ny - dx; y++)
+      for (int z = lo; z <= o.nz - dx; z++) {
+        const size_t L = o.lin(x, y, z);
+        if (o.walls_all[L] > 0) continue;
+        if (o.rhoN[L] > 0.0) {
+          epv = epv + (o.rho[L] - o.p.rho0) / 3.0;
+          emov = emov + 0.5 * o.rho[L] * (sq(o.ux[L]) + sq(o.uy[L]) + sq(o.uz[L]));
+        }
+        for (int i = 1; i < 19; i++) {
+          int xn = x + CIX[i], yn = y + CIY[i], zn = z + CIZ[i];
+          if (!o.ref) { xn = Orc::wrap(xn, o.nx); yn = Orc::wrap(yn, o.ny); zn = Orc::wrap(zn, o.nz); }
+          const size_t Ln = o.lin(xn, yn, zn);
+          if (o.rhoN[L] * o.rhoN[Ln] < 0.0 && o.walls_all[Ln] <= 0) {
+            area = area + 1.0;
+            break;
+          }
+        }
+      }
+  out[0] = epv;
+  out[1] = emov;
+  out[2] = area;
+}
+
 // CONFIG stop rule: min_z sqrt(sum_xy (1+phi)/2 / pi), phi = rho_N after calmacros
 double orc_neck_radius(void* h) {
   Orc& o = *(Orc*)h;

@@ -59,6 +59,13 @@ def lib() -> ctypes.CDLL:
         L.sym_get_field.argtypes = [H, ctypes.c_int, ctypes.c_void_p]
         L.sym_set_populations.argtypes = [H, ctypes.c_void_p, ctypes.c_void_p]
         L.sym_get_macros.argtypes = [H] + [ctypes.c_void_p] * 5
+        L.sym_energy.argtypes = [H, ctypes.c_void_p]
+        L.sym_output_results.argtypes = [H, ctypes.c_char_p]
+        L.sym_output_result2.argtypes = [H, ctypes.c_char_p, ctypes.c_int, ctypes.c_double]
+        L.sym_output3_write.argtypes = [H, ctypes.c_char_p, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                        ctypes.c_double]
+        L.sym_output4.argtypes = [H, ctypes.c_char_p, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                  ctypes.POINTER(ctypes.c_double)]
         L.sym_checkpoint_save.argtypes = [H, ctypes.c_char_p]
         L.sym_checkpoint_load.argtypes = [H, ctypes.c_char_p]
         L.sym_set_particles.argtypes = [H, ctypes.POINTER(SymParticles)]
@@ -176,6 +183,27 @@ class Lattice:
                 raise ValueError(f"{k}: contiguous float64 array of {self.p.n_nodes} values expected")
         self._ck(lib().sym_get_macros(self.h, *(out[k].ctypes.data for k in names)), "get_macros")
         return out
+
+    def energy(self) -> np.ndarray:
+        """output4's sums before normalisation (see sym_energy)."""
+        out = np.zeros(6)
+        self._ck(lib().sym_energy(self.h, out.ctypes.data), "energy")
+        return out
+
+    def output_results(self, path: str):
+        self._ck(lib().sym_output_results(self.h, os.fsencode(path)), "output_results")
+
+    def output_result2(self, prefix: str, t: int, tr: float):
+        self._ck(lib().sym_output_result2(self.h, os.fsencode(prefix), t, tr), "output_result2")
+
+    def output3_write(self, path: str, t: int, tr: float, rad_c: float, lamda_d: float):
+        self._ck(lib().sym_output3_write(self.h, os.fsencode(path), t, tr, rad_c, lamda_d), "output3")
+
+    def output4(self, path: str, t: int, tr: float, rad_c: float, wcap: float) -> float:
+        """Append the Energy.dat record; returns the accumulated capillary work."""
+        w = ctypes.c_double(wcap)
+        self._ck(lib().sym_output4(self.h, os.fsencode(path), t, tr, rad_c, ctypes.byref(w)), "output4")
+        return w.value
 
     def save(self, path: str):
         """Checkpoint the complete stepping state to `path`."""
