@@ -76,7 +76,8 @@ typedef struct sym_params {
   int32_t storage;      /* SYM_STORE_* used by sym_step in CONFIG mode            */
   int32_t par;          /* number of particles, 0..SYM_MAX_PAR (:24)              */
   int32_t la_m, la_n;   /* Lagrange grid La_m, La_n (:87-88); 0 = from alpha      */
-  int32_t reserved0;
+  int32_t bounce;       /* moving-particle bounce-back: 0 halfway (curve, :990-1034),
+                           1 interpolated with the link fraction (curve2, :1036-1101) */
   double rho0;          /* reference density (:67); solid-node rho (:788)         */
   double nu_r, nu_b;    /* kinematic viscosities of red/blue (:69-70)             */
   /* MRT rates. A value <= 0 selects the reference's node-local rate

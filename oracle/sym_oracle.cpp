@@ -656,6 +656,74 @@ void curve(Orc& o) {
   }
 }
 
+// curve2 (Source1.f90:1036-1101): moving-particle bounce-back interpolated with
+// the link fraction qq (the distance from the node to the sphere along the link
+// over the link length), the wall velocity taken at the wall point.  Links into
+// CONFIG wall planes keep the halfway bounce-back of curve.  One node's links
+// are updated in index order, as in the reference's loop (a link may read a
+// population of the same node updated before it).
+void curve2(Orc& o) {
+#pragma omp parallel for schedule(static)
+  for (int x = o.lo_x; x <= o.hi_x; x++)
+    for (int y = o.lo_y; y <= o.hi_y; y++)
+      for (int z = o.lo_z; z <= o.hi_z; z++) {
+        const size_t L = o.lin(x, y, z);
+        const int pp = o.pout[L];
+        if (pp < 1) continue;
+        for (int i = 1; i < 19; i++) {
+          const int xb = o.ref ? x - CIX[i] : Orc::wrap(x - CIX[i], o.nx);
+          const int yb = o.ref ? y - CIY[i] : Orc::wrap(y - CIY[i], o.ny);
+          const int zb = o.ref ? z - CIZ[i] : Orc::wrap(z - CIZ[i], o.nz);
+          const size_t B = o.lin(xb, yb, zb);
+          const int wb = o.walls[B];
+          if (wb == pp && pp <= o.par) {
+            const int xf = o.ref ? x + CIX[i] : Orc::wrap(x + CIX[i], o.nx);
+            const int yf = o.ref ? y + CIY[i] : Orc::wrap(y + CIY[i], o.ny);
+            const int zf = o.ref ? z + CIZ[i] : Orc::wrap(z + CIZ[i], o.nz);
+            const size_t F = o.lin(xf, yf, zf);
+            const double cx = CIX[i], cy = CIY[i], cz = CIZ[i];
+            const double x0 = o.disp(o.coord(x), o.C(o.s.center, pp, 0), 0);
+            const double y0 = o.disp(o.coord(y), o.C(o.s.center, pp, 1), 1);
+            const double z0 = o.disp(o.coord(z), o.C(o.s.center, pp, 2), 2);
+            double star = cx * x0 + cy * y0 + cz * z0;
+            const double R2 = o.p.rad * o.p.rad;
+            double star1 = cx * cx * (R2 - y0 * y0 - z0 * z0) + cy * cy * (R2 - x0 * x0 - z0 * z0) +
+                           cz * cz * (R2 - x0 * x0 - y0 * y0);
+            star1 = star1 + 2.0 * (cx * cy * x0 * y0 + cy * cz * y0 * z0 + cz * cx * z0 * x0);
+            star1 = std::sqrt(star1);
+            const double star2 = cx * cx + cy * cy + cz * cz;
+            const double xw = x0 + cx * (star1 - star) / star2;
+            const double yw = y0 + cy * (star1 - star) / star2;
+            const double zw = z0 + cz * (star1 - star) / star2;
+            const double dis = sq(xw - x0) + sq(yw - y0) + sq(zw - z0);
+            const double qq = std::sqrt(dis) / std::sqrt(star2);
+            const double xr = o.disp(o.coord(x) - cx * qq, o.C(o.s.center, pp, 0), 0);
+            const double yr = o.disp(o.coord(y) - cy * qq, o.C(o.s.center, pp, 1), 1);
+            const double zr = o.disp(o.coord(z) - cz * qq, o.C(o.s.center, pp, 2), 2);
+            double uw[3];
+            rigid_u(o, o.s.center, pp, xr, yr, zr, uw);
+            star = uw[0] * cx + uw[1] * cy + uw[2] * cz;
+            const int j = OPC[i];
+            o.ri[19 * L + i] = 1.0 / (1.0 + qq) *
+                               (qq * (o.ri[19 * F + i] + o.ri[19 * B + j]) + (1.0 - qq) * o.ri[19 * L + j] +
+                                6.0 * o.wi[i] * o.rhoR[L] * star);
+            o.bi[19 * L + i] = 1.0 / (1.0 + qq) *
+                               (qq * (o.bi[19 * F + i] + o.bi[19 * B + j]) + (1.0 - qq) * o.bi[19 * L + j] +
+                                6.0 * o.wi[i] * o.rhoB[L] * star);
+          } else if (wb == pp || (!o.ref && wb > o.par)) {
+            // halfway (curve) for the CONFIG wall planes
+            o.ri[19 * L + i] = o.ri[19 * B + OPC[i]];
+            o.bi[19 * L + i] = o.bi[19 * B + OPC[i]];
+          }
+        }
+      }
+  if (o.ref) {
+    sym_fi_x(o, o.ri); sym_fi_x(o, o.bi);
+    sym_fi_y(o, o.ri); sym_fi_y(o, o.bi);
+    sym_fi_z(o, o.ri); sym_fi_z(o, o.bi);
+  }
+}
+
 // momentum (Source1.f90:1178-1261): Galilean-invariant momentum exchange.
 // Per-x-plane partial sums combined in x order (deterministic for any thread count).
 void momentum(Orc& o) {
@@ -1057,7 +1125,8 @@ void step(Orc& o) {
   boundary(o);
   streaming(o, o.ri);
   streaming(o, o.bi);
-  curve(o);
+  if (o.p.bounce) curve2(o);
+  else curve(o);
 }
 
 }  // namespace
@@ -1157,7 +1226,11 @@ void orc_collision(void* h) { collision(*(Orc*)h); }
 void orc_recolor(void* h) { recolor(*(Orc*)h); }
 void orc_boundary(void* h) { boundary(*(Orc*)h); }
 void orc_streaming(void* h, int which) { Orc* o = (Orc*)h; streaming(*o, which == 0 ? o->ri : o->bi); }
-void orc_curve(void* h) { curve(*(Orc*)h); }
+void orc_curve(void* h) {
+  Orc& o = *(Orc*)h;
+  if (o.p.bounce) curve2(o);
+  else curve(o);
+}
 void orc_lagrange_points(void* h) { lagrange_points(*(Orc*)h); }
 void orc_capillary_force2(void* h) { capillary_force2(*(Orc*)h); }
 void orc_momentum(void* h) { momentum(*(Orc*)h); }

@@ -216,6 +216,7 @@ int enqueue_batch_step(sym_batch* b, int k, cudaEvent_t* ev) {
   using R = typename Codec<S>::R;
   k_collide_batch<S><<<b->grid, kTPB, smem_bytes<S>(), b->st>>>(b->d_desc[k], b->d_tiles, b->ntiles,
                                                                   b->d_counter + k);
+  if (int e = sparse_enqueue_post(b->sparse, k, b->st)) return berr(b, e, "interpolated bounce-back");
   if (ev) cudaEventRecord(ev[3], b->st);
   return bcuda(b, cudaGetLastError(), "batch step");
 }

@@ -75,6 +75,7 @@ void fill_devparams(const sym_params& p, DevParams& d) {
   d.s_e = p.s_e; d.s_eps = p.s_eps; d.s_q = p.s_q; d.s_pi = p.s_pi; d.s_m = p.s_m;
   d.sigma = p.sigma; d.beta = p.beta; d.cita = p.cita;
   d.sin_cita = std::sin(p.cita); d.cos_cita = std::cos(p.cita);
+  d.bounce = p.bounce;
   for (int k = 0; k < 3; k++) d.body[k] = p.body[k];
   d.rad = p.rad;
   d.mass = p.mass > 0 ? p.mass : 4.0 / 3.0 * p.rho_p * M_PI * (p.rad * p.rad * p.rad);
@@ -145,12 +146,16 @@ int32_t* field_ptr_i(sym_handle* h, int f) {
   }
 }
 
-// Allocate the canonical arrays a CONFIG handle defers (fi, ffi, ft).
+// Allocate the canonical arrays a CONFIG handle defers (fi, ffi, ft).  With
+// the interpolated particle bounce-back the fused path also keeps the red
+// post-collision populations of the nodes next to particles behind ffi
+// (ffi + 19N), for the link update after the collide kernel.
 int ensure_full(sym_handle* h) {
   double** pops[3] = {&h->fi, &h->ffi, &h->ft};
+  const bool rpost = h->p.mode == SYM_MODE_CONFIG && h->p.bounce && h->p.par > 0;
   for (auto pp : pops)
     if (!*pp)
-      if (int e = dalloc(h, pp, 19 * h->N)) return e;
+      if (int e = dalloc(h, pp, (pp == &h->ffi && rpost ? 38 : 19) * h->N)) return e;
   return SYM_OK;
 }
 
@@ -281,6 +286,7 @@ int sym_params_check(const sym_params* p, char* msg, size_t msg_len) {
   if (p->mode != SYM_MODE_REFERENCE && p->mode != SYM_MODE_CONFIG) return fail("unknown mode");
   if (p->storage < SYM_STORE_FP64 || p->storage > SYM_STORE_FP16) return fail("unknown storage");
   if (p->par < 0 || p->par > SYM_MAX_PAR) return fail("par out of range");
+  if (p->bounce != 0 && p->bounce != 1) return fail("bounce must be 0 (halfway) or 1 (interpolated)");
   if (!(p->nu_r > 0.0) || !(p->nu_b > 0.0) || !std::isfinite(p->nu_r) || !std::isfinite(p->nu_b))
     return fail("viscosities must be finite and > 0 (tau > 0.5)");
   if (!(p->rho0 > 0.0) || !std::isfinite(p->rho0)) return fail("rho0 must be finite and > 0");

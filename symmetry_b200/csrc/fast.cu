@@ -111,6 +111,7 @@ int enqueue_step(sym_handle* h, int cur, int pc, cudaEvent_t* ev) {
     k_collide<S, false><<<grid, TPB, shm, h->st>>>(P, pd, pin_, pnext, phic, h->walls, h->walls_all, h->pout,
                                                    h->dpart, h->ffi, rr_old(h, pc), rr_new(h, pc), accbuf<S>(h),
                                                    h->fast.status, tp, tr, xc);
+  if (int e = sparse_enqueue_post(h->fast.sparse, cur, h->st)) return set_error(h, e, "interpolated bounce-back");
   if (ev) cudaEventRecord(ev[3], h->st);
   return check_cuda(h, cudaGetLastError(), "fast step");
 }

@@ -525,6 +525,9 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
         const unsigned T = L + (CX(i) > 0 ? oxp : (CX(i) < 0 ? oxm : 0)) +
                            (CY(i) > 0 ? oyp : (CY(i) < 0 ? oym : 0)) + (CZ(i) > 0 ? ozp : (CZ(i) < 0 ? ozm : 0));
         if (!act) return;
+        // interpolated bounce-back: the red post-collision populations of the
+        // nodes next to particles, for the link update after this kernel
+        if (SOLIDX && P.bounce && pp >= 1 && pp <= P.par) ffi[(size_t)(19 + i) * N + L] = (double)r;
         if (SOLIDX && i > 0 && pp >= 1) {
           const int wb = walls[T];
           const bool flat = wb > P.par;

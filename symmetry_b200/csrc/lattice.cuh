@@ -89,6 +89,7 @@ struct DevParams {
   int lo[3], hi[3];        // update range, 0-based inclusive, per axis (x,y,z)
   int wall_x;
   int par, la_m, la_n, la_num;
+  int bounce;              // 0 halfway bounce-back (curve), 1 interpolated (curve2)
   double rho0, nu_r, nu_b;
   double s_e, s_eps, s_q, s_pi, s_m;
   double sigma, beta, cita;
@@ -341,6 +342,26 @@ __device__ __forceinline__ void mrt_collide_pairs(const DevParams& P, R f[19], R
     f[i] = e + o;
     f[OPC(i)] = e - o;
   });
+}
+
+// Link fraction of curve2 (Source1.f90:1055-1070): node at displacement
+// (x0,y0,z0) from the centre of a sphere of radius rad, link c pointing out of
+// the sphere: qq = distance from the node back along -c to the sphere surface,
+// over |c|.
+__device__ __forceinline__ double link_fraction(double x0, double y0, double z0, double cx, double cy, double cz,
+                                                double rad) {
+  const double star = cx * x0 + cy * y0 + cz * z0;
+  const double R2 = rad * rad;
+  double star1 = cx * cx * (R2 - y0 * y0 - z0 * z0) + cy * cy * (R2 - x0 * x0 - z0 * z0) +
+                 cz * cz * (R2 - x0 * x0 - y0 * y0);
+  star1 = star1 + 2.0 * (cx * cy * x0 * y0 + cy * cz * y0 * z0 + cz * cx * z0 * x0);
+  star1 = sqrt(star1);
+  const double star2 = cx * cx + cy * cy + cz * cz;
+  const double xw = x0 + cx * (star1 - star) / star2;
+  const double yw = y0 + cy * (star1 - star) / star2;
+  const double zw = z0 + cz * (star1 - star) / star2;
+  const double dis = (xw - x0) * (xw - x0) + (yw - y0) * (yw - y0) + (zw - z0) * (zw - z0);
+  return sqrt(dis) / sqrt(star2);
 }
 
 __device__ __forceinline__ void unitization(double a[3]) {

@@ -359,6 +359,58 @@ __global__ void k_curve(DevParams P, const sym_particles* __restrict__ S, const 
   }
 }
 
+// curve2 (Source1.f90:1036-1101): bounce-back interpolated with the link
+// fraction, the wall velocity at the wall point; one thread per node updates
+// its links in index order like the reference's loop.  CONFIG wall planes keep
+// the halfway bounce-back.
+__global__ void k_curve2(DevParams P, const sym_particles* __restrict__ S, const int32_t* __restrict__ walls,
+                         const int32_t* __restrict__ pout, double* ri, double* bi, const double* __restrict__ rhoR,
+                         const double* __restrict__ rhoB) {
+  int x, y, z;
+  if (!range_node(P, blockIdx.x * (long long)blockDim.x + threadIdx.x, x, y, z)) return;
+  const long long L = lin(P, x, y, z), N = P.N;
+  const int pp = pout[L];
+  if (pp < 1) return;
+  const int par = P.par;
+#pragma unroll 1
+  for (int i = 1; i < 19; i++) {
+    const int xb = P.ref ? x - CX(i) : wrapi(x - CX(i), P.nx);
+    const int yb = P.ref ? y - CY(i) : wrapi(y - CY(i), P.ny);
+    const int zb = P.ref ? z - CZ(i) : wrapi(z - CZ(i), P.nz);
+    const long long B = lin(P, xb, yb, zb);
+    const int wb = walls[B];
+    const int j = OPC(i);
+    if (wb == pp && pp <= par) {
+      const int xf = P.ref ? x + CX(i) : wrapi(x + CX(i), P.nx);
+      const int yf = P.ref ? y + CY(i) : wrapi(y + CY(i), P.ny);
+      const int zf = P.ref ? z + CZ(i) : wrapi(z + CZ(i), P.nz);
+      const long long F = lin(P, xf, yf, zf);
+      const double cx = CX(i), cy = CY(i), cz = CZ(i);
+      const double* c = S->center;
+      const double x0 = disp(P, (double)(x + P.origin), c[0 * par + pp - 1], 0);
+      const double y0 = disp(P, (double)(y + P.origin), c[1 * par + pp - 1], 1);
+      const double z0 = disp(P, (double)(z + P.origin), c[2 * par + pp - 1], 2);
+      const double qq = link_fraction(x0, y0, z0, cx, cy, cz, P.rad);
+      const double xr = disp(P, (double)(x + P.origin) - cx * qq, c[0 * par + pp - 1], 0);
+      const double yr = disp(P, (double)(y + P.origin) - cy * qq, c[1 * par + pp - 1], 1);
+      const double zr = disp(P, (double)(z + P.origin) - cz * qq, c[2 * par + pp - 1], 2);
+      const double* up = S->up;
+      const double* rp = S->rp;
+      const double uw0 = up[0 * par + pp - 1] + zr * rp[1 * par + pp - 1] - yr * rp[2 * par + pp - 1];
+      const double uw1 = up[1 * par + pp - 1] + xr * rp[2 * par + pp - 1] - zr * rp[0 * par + pp - 1];
+      const double uw2 = up[2 * par + pp - 1] + yr * rp[0 * par + pp - 1] - xr * rp[1 * par + pp - 1];
+      const double star = uw0 * cx + uw1 * cy + uw2 * cz;
+      ri[i * N + L] = 1.0 / (1.0 + qq) *
+                      (qq * (ri[i * N + F] + ri[j * N + B]) + (1.0 - qq) * ri[j * N + L] + 6.0 * W(i) * rhoR[L] * star);
+      bi[i * N + L] = 1.0 / (1.0 + qq) *
+                      (qq * (bi[i * N + F] + bi[j * N + B]) + (1.0 - qq) * bi[j * N + L] + 6.0 * W(i) * rhoB[L] * star);
+    } else if (wb == pp || (!P.ref && wb > par)) {
+      ri[i * N + L] = ri[j * N + B];
+      bi[i * N + L] = bi[j * N + B];
+    }
+  }
+}
+
 // ---- initial state -----------------------------------------------------------
 // initialization (Source1.f90:850-896), REFERENCE geometry
 __global__ void k_initialization(DevParams P, double* rhoN, double* rho, double* rhoR, double* rhoB, double* ux,
@@ -604,8 +656,12 @@ int ref_streaming(sym_handle* h, int which) {
 
 int ref_curve(sym_handle* h) {
   const DevParams& P = h->dp;
-  k_curve<<<blocks_for(range_count(P)), TPB, 0, h->st>>>(P, h->dpart, h->walls, h->pout, h->ri, h->bi, h->rhoR,
-                                                          h->rhoB);
+  if (P.bounce)
+    k_curve2<<<blocks_for(range_count(P)), TPB, 0, h->st>>>(P, h->dpart, h->walls, h->pout, h->ri, h->bi, h->rhoR,
+                                                             h->rhoB);
+  else
+    k_curve<<<blocks_for(range_count(P)), TPB, 0, h->st>>>(P, h->dpart, h->walls, h->pout, h->ri, h->bi, h->rhoR,
+                                                            h->rhoB);
   if (P.ref)
     for (int ax = 0; ax < 3; ax++) { mirror_pop(h, h->ri, ax); mirror_pop(h, h->bi, ax); }
   return check_cuda(h, cudaGetLastError(), "curve");

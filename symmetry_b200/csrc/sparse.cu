@@ -17,6 +17,9 @@
 //                   planes, sphere marks, pin/pout
 //   refilling       uncovered nodes (:1351-1418), then into the fused state
 //   pin fill        fictitious phi on solid nodes next to fluid
+// and, after the collide kernel, with the interpolated bounce-back:
+//   curve2          links into a particle re-set with the link fraction
+//                   (:1036-1101)
 // Masks, refills and sums are written per particle in the same order as the
 // per-handle kernels of particles.cu, so results are those of the drop-in
 // path bit for bit.
@@ -51,6 +54,10 @@ struct SpDom {
   void* phic;            // this step's phase field (pin-filled below)
   void* phip;            // the previous step's phase field
   const float* rr_old;   // 16-bit storage: 1/rho_ref of the populations
+  void* pnext;           // the populations this step's collide kernel writes
+  const float* rr_cur;   // 16-bit storage: 1/rho_ref they are encoded with
+  void* acc;             // next step's accumulated colour densities
+  int* status;
   Box bprep, bmom, bmark, bpin, bref, bpfill;
   long long nblk_mom;
   int full_reset;        // more than one particle: masks reset on the whole domain
@@ -221,6 +228,72 @@ __global__ void __launch_bounds__(kT) k_sp_pinfill_box(const SpDom* __restrict__
   pinfill_node<R>(D.P, D.pd, (R*)D.phic, D.pin, D.walls_all, x, y, z);
 }
 
+// curve2 (Source1.f90:1036-1101) on the fused state, after the collide kernel:
+// the collide kernel bounced every link into particle pp halfway (curve) and
+// kept the node's red post-collision populations behind ffi; here each such
+// link of a node next to pp is replaced, in index order, by the
+// interpolation of the reference with link fraction qq:
+//   r_i = [qq (r*_i(x) + r*_opc(x)) + (1-qq) r_opc(x) + 6 w_i rhoR(x) uw.c_i] / (1+qq)
+// with r* the node's post-collision values and r_opc(x) the population that
+// arrived from x + c_i; likewise for blue.  The change of each updated
+// population is added to the node's accumulated densities.
+template <typename S>
+__global__ void __launch_bounds__(kT) k_sp_curve2(const SpDom* __restrict__ doms, const Blk* __restrict__ map) {
+  using R = typename Codec<S>::R;
+  const Blk e = map[blockIdx.x];
+  const SpDom& D = doms[e.d];
+  const DevParams& P = D.P;
+  const int pp = e.pp, par = P.par;
+  int x, y, z;
+  if (!part::box_node(P, D.bmom, D.S->center, pp, (long long)e.b * kT + threadIdx.x, x, y, z)) return;
+  const long long L = lin(P, x, y, z);
+  if (D.pout[L] != pp) return;
+  const unsigned N = (unsigned)P.N;
+  const double* ff = D.ffi;
+  const double* rp = D.ffi + 19 * (size_t)N;
+  const R irr = Codec<S>::kRef ? R(D.rr_cur[D.pd.idx(x, y, z)]) : R(1.0 / P.rho0);
+  const R rref = Codec<S>::kRef ? R(1) / irr : R(P.rho0);
+  S* pops = (S*)D.pnext;
+  const double* c = D.S->center;
+  const double x0 = disp(P, (double)(x + P.origin), c[0 * par + pp - 1], 0);
+  const double y0 = disp(P, (double)(y + P.origin), c[1 * par + pp - 1], 1);
+  const double z0 = disp(P, (double)(z + P.origin), c[2 * par + pp - 1], 2);
+  const double rhoR = D.rhoR[L], rhoB = D.rhoB[L];
+  double dr = 0.0, db = 0.0;
+  static_for<18>([&](auto ic) {
+    constexpr int i = decltype(ic)::value + 1;
+    constexpr int j = OPC(i);
+    const long long B = lin(P, wrapi(x - CX(i), P.nx), wrapi(y - CY(i), P.ny), wrapi(z - CZ(i), P.nz));
+    if (D.walls[B] != pp) return;
+    const double cx = CX(i), cy = CY(i), cz = CZ(i);
+    const double qq = link_fraction(x0, y0, z0, cx, cy, cz, P.rad);
+    const double xr = disp(P, (double)(x + P.origin) - cx * qq, c[0 * par + pp - 1], 0);
+    const double yr = disp(P, (double)(y + P.origin) - cy * qq, c[1 * par + pp - 1], 1);
+    const double zr = disp(P, (double)(z + P.origin) - cz * qq, c[2 * par + pp - 1], 2);
+    const double* up = D.S->up;
+    const double* rw = D.S->rp;
+    const double uw0 = up[0 * par + pp - 1] + zr * rw[1 * par + pp - 1] - yr * rw[2 * par + pp - 1];
+    const double uw1 = up[1 * par + pp - 1] + xr * rw[2 * par + pp - 1] - zr * rw[0 * par + pp - 1];
+    const double uw2 = up[2 * par + pp - 1] + yr * rw[0 * par + pp - 1] - xr * rw[1 * par + pp - 1];
+    const double star = uw0 * cx + uw1 * cy + uw2 * cz;
+    const double ar = rp[(size_t)i * N + L], br = rp[(size_t)j * N + L];
+    const double ab = ff[(size_t)i * N + L] - ar, bb = ff[(size_t)j * N + L] - br;
+    R cr, cb, hr, hb;
+    Codec<S>::template load<j>(pops, N, (unsigned)L, rref, cr, cb);
+    Codec<S>::template load<i>(pops, N, (unsigned)L, rref, hr, hb);
+    const double vr = 1.0 / (1.0 + qq) * (qq * (ar + br) + (1.0 - qq) * (double)cr + 6.0 * W(i) * rhoR * star);
+    const double vb = 1.0 / (1.0 + qq) * (qq * (ab + bb) + (1.0 - qq) * (double)cb + 6.0 * W(i) * rhoB * star);
+    Codec<S>::template store<i>(pops, N, (unsigned)L, irr, R(vr), R(vr) + R(vb));
+    dr += vr - (double)hr;
+    db += vb - (double)hb;
+  });
+  using AT = typename Acc<R>::T;
+  if (dr != 0.0 || db != 0.0) {
+    acc_add<R>((AT*)D.acc + L, R(dr), D.status);
+    acc_add<R>((AT*)D.acc + P.N + L, R(db), D.status);
+  }
+}
+
 long long nblocks(long long n) { return (n + kT - 1) / kT; }
 
 }  // namespace
@@ -231,7 +304,7 @@ struct SparsePlan {
   SpDom* d_dom[2] = {nullptr, nullptr};   // per parity
   // block tables, one per launch; several launches per particle index keep
   // the per-particle order of the masks and refills
-  enum { PREP, LAG, CAP, CAPF, MOM, MOMF, RESET, FLAT, PINPLANE, PFPLANE, PFBOX, NFIX };
+  enum { PREP, LAG, CAP, CAPF, MOM, MOMF, RESET, FLAT, PINPLANE, PFPLANE, PFBOX, CURVE2, NFIX };
   struct Table {
     Blk* d = nullptr;
     int n = 0;
@@ -275,6 +348,10 @@ SpDom make_dom(sym_handle* h, int cur, int pc) {
   d.phic = phip(h, pc);
   d.phip = phip(h, 1 - pc);
   d.rr_old = h->fast.rref[1 - pc];
+  d.pnext = popp(h, 1 - cur);
+  d.rr_cur = h->fast.rref[pc];
+  d.acc = h->fast.acc;
+  d.status = h->fast.status;
   d.bprep = part::sphere_box(h->dp, 6.0);
   d.bmom = part::sphere_box(h->dp, 3.0);
   d.bmark = part::sphere_box(h->dp, 1.0);
@@ -343,6 +420,8 @@ SparsePlan* sparse_plan_build(const std::vector<sym_handle*>& doms, const std::v
       for (long long b = 0; b < D.nblk_mom; b++) tb[SparsePlan::MOM].push_back({i, pp, (int)b, 0});
       tb[SparsePlan::MOMF].push_back({i, pp, 0, 0});
       for (long long b = 0; b < nblocks(D.bpfill.count()); b++) tb[SparsePlan::PFBOX].push_back({i, pp, (int)b, 0});
+      if (P.bounce)
+        for (long long b = 0; b < nblocks(D.bmom.count()); b++) tb[SparsePlan::CURVE2].push_back({i, pp, (int)b, 0});
     }
   }
   std::vector<std::vector<Blk>> mk(maxpar), pn(maxpar), rf(maxpar);
@@ -425,6 +504,26 @@ void enqueue_plan(SparsePlan* p, int k, cudaStream_t st) {
   go(k_sp_pinfill_box<R>, f[SparsePlan::PFBOX]);
 }
 }  // namespace
+
+namespace {
+template <typename S>
+void enqueue_post(SparsePlan* p, int k, cudaStream_t st) {
+  const auto& t = p->fix[SparsePlan::CURVE2];
+  if (t.n) k_sp_curve2<S><<<t.n, kT, 0, st>>>(p->d_dom[k], t.d);
+}
+}  // namespace
+
+// the work after the collide kernel of step parity k (the interpolated
+// particle bounce-back), on `st`
+int sparse_enqueue_post(SparsePlan* p, int k, cudaStream_t st) {
+  if (!p || p->storage < 0 || !p->fix[SparsePlan::CURVE2].n) return SYM_OK;
+  switch (p->storage) {
+    case SYM_STORE_FP64: enqueue_post<double>(p, k, st); break;
+    case SYM_STORE_FP32: enqueue_post<float>(p, k, st); break;
+    default: enqueue_post<__half>(p, k, st);
+  }
+  return cudaGetLastError() == cudaSuccess ? SYM_OK : SYM_ERR_CUDA;
+}
 
 // the sparse work of step parity k on `st` (graph-capturable: no host sync)
 int sparse_enqueue(SparsePlan* p, int k, cudaStream_t st) {

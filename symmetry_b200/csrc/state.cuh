@@ -127,6 +127,7 @@ int fast_neck_planes(sym_handle* h, double* out, cudaStream_t st);   // per-z re
 SparsePlan* sparse_plan_build(const std::vector<sym_handle*>& doms, const std::vector<int>& cur0,
                               const std::vector<int>& pc0, cudaStream_t st, int* err);
 int sparse_enqueue(SparsePlan* p, int k, cudaStream_t st);
+int sparse_enqueue_post(SparsePlan* p, int k, cudaStream_t st);   // after the collide kernel
 int sparse_launches(const SparsePlan* p);
 void sparse_plan_free(SparsePlan* p);
 

@@ -21,7 +21,7 @@ module symmetry_gpu
   integer, parameter :: SYM_MAX_PAR = 32
 
   type, bind(C) :: sym_params
-     integer(c_int32_t) :: nx, ny, nz, mode, wall_x, storage, par, la_m, la_n, reserved0
+     integer(c_int32_t) :: nx, ny, nz, mode, wall_x, storage, par, la_m, la_n, bounce
      real(c_double) :: rho0, nu_r, nu_b, s_e, s_eps, s_q, s_pi, s_m, sigma, beta, cita
      real(c_double) :: body(3)
      real(c_double) :: rad, rho_p, mass, inertia, fg, alpha, evap_lim

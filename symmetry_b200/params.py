@@ -38,7 +38,7 @@ class SymParams(ctypes.Structure):
         ("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32),
         ("mode", ctypes.c_int32), ("wall_x", ctypes.c_int32), ("storage", ctypes.c_int32),
         ("par", ctypes.c_int32), ("la_m", ctypes.c_int32), ("la_n", ctypes.c_int32),
-        ("reserved0", ctypes.c_int32),
+        ("bounce", ctypes.c_int32),
         ("rho0", ctypes.c_double), ("nu_r", ctypes.c_double), ("nu_b", ctypes.c_double),
         ("s_e", ctypes.c_double), ("s_eps", ctypes.c_double), ("s_q", ctypes.c_double),
         ("s_pi", ctypes.c_double), ("s_m", ctypes.c_double),

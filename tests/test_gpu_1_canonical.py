@@ -34,15 +34,22 @@ def small_c1():
     return configs.c1_thread(nx=16, ny=16, nz=48, radius=4.0)
 
 
+def small_c2_interp():
+    w = small_c2()
+    w.params.bounce = 1   # curve2, Source1.f90:1036-1101
+    return w
+
+
 def cases():
     return {
         "c1": lambda: orc_setup(small_c1()),
         "c2": lambda: orc_setup(small_c2()),
+        "c2_interp": lambda: orc_setup(small_c2_interp()),
         "ref": lambda: setup_reference(params.reference_params(48, 88, 48)),
     }
 
 
-@pytest.mark.parametrize("case", ["c1", "c2", "ref"])
+@pytest.mark.parametrize("case", ["c1", "c2", "c2_interp", "ref"])
 def test_subroutine_parity(case):
     o = cases()[case]()
     L = Lattice(o.p)

@@ -79,6 +79,19 @@ def test_fast_fp64_c2_walls_particle_300_steps():
     compare_particles(o, L, 1, 1e-9, ["center", "up", "rp"])
 
 
+def test_fast_fp64_c2_interpolated_bounce_back_300_steps():
+    """The moving sphere with the interpolated bounce-back of curve2
+    (Source1.f90:1036-1101) in the fused path against the oracle."""
+    w = configs.c2_wall_particle(nx=32, ny=32, nz=64, rad=5.0, centre=(16.0, 16.0, 20.0), z0=20.0, z1=44.0)
+    w.params.bounce = 1
+    o, L = fast_run(w, 300)
+    fluid = o.arr("walls_all") == 0
+    e = errors(o, L, mask=fluid)
+    assert max(e.values()) <= 1e-10, e
+    compare_masks(o, L, ["walls", "walls_all", "pin", "pout"])
+    compare_particles(o, L, 1, 1e-9, ["center", "up", "rp"])
+
+
 def test_fast_fp64_c2_full_size_100_steps():
     """configs[1] at its full 64x64x128 size (short run)."""
     w = configs.c2_wall_particle()
