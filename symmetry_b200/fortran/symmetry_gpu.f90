@@ -88,6 +88,54 @@ module symmetry_gpu
        real(c_double), intent(out) :: hmin
        integer(c_int32_t), intent(out) :: y0
      end function
+     ! output steps (Source1.f90:218-234); paths are NUL-terminated character arrays
+     integer(c_int) function sym_get_macros(h, rho, ux, uy, uz, rho_n) bind(C, name="sym_get_macros")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h, rho, ux, uy, uz, rho_n
+     end function
+     integer(c_int) function sym_energy(h, out) bind(C, name="sym_energy")
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       real(c_double), intent(out) :: out(6)
+     end function
+     integer(c_int) function sym_output_results(h, path) bind(C, name="sym_output_results")
+       import :: c_int, c_ptr, c_char
+       type(c_ptr), value :: h
+       character(kind=c_char), intent(in) :: path(*)
+     end function
+     integer(c_int) function sym_output_result2(h, prefix, t, tr) bind(C, name="sym_output_result2")
+       import :: c_int, c_ptr, c_char, c_double
+       type(c_ptr), value :: h
+       character(kind=c_char), intent(in) :: prefix(*)
+       integer(c_int), value :: t
+       real(c_double), value :: tr
+     end function
+     integer(c_int) function sym_output3_write(h, path, t, tr, rad_c, lamda_d) bind(C, name="sym_output3_write")
+       import :: c_int, c_ptr, c_char, c_double
+       type(c_ptr), value :: h
+       character(kind=c_char), intent(in) :: path(*)
+       integer(c_int), value :: t
+       real(c_double), value :: tr, rad_c, lamda_d
+     end function
+     integer(c_int) function sym_output4(h, path, t, tr, rad_c, wcap_acc) bind(C, name="sym_output4")
+       import :: c_int, c_ptr, c_char, c_double
+       type(c_ptr), value :: h
+       character(kind=c_char), intent(in) :: path(*)
+       integer(c_int), value :: t
+       real(c_double), value :: tr, rad_c
+       real(c_double), intent(inout) :: wcap_acc
+     end function
+     ! checkpoint / restart (no counterpart in the reference)
+     integer(c_int) function sym_checkpoint_save(h, path) bind(C, name="sym_checkpoint_save")
+       import :: c_int, c_ptr, c_char
+       type(c_ptr), value :: h
+       character(kind=c_char), intent(in) :: path(*)
+     end function
+     integer(c_int) function sym_checkpoint_load(h, path) bind(C, name="sym_checkpoint_load")
+       import :: c_int, c_ptr, c_char
+       type(c_ptr), value :: h
+       character(kind=c_char), intent(in) :: path(*)
+     end function
   end interface
 
   ! one binding per reference subroutine (Source1.f90 names)
