@@ -74,6 +74,13 @@ struct Codec<double> {
     r = v.x;
     b = v.y;
   }
+  // total f = r + b and red r
+  template <int I>
+  __device__ __forceinline__ static void load_fr(const double* __restrict__ p, unsigned N, unsigned L, R, R& f, R& r) {
+    const double2 v = reinterpret_cast<const double2*>(p)[I * N + L];
+    r = v.x;
+    f = v.x + v.y;
+  }
   template <int I>
   __device__ __forceinline__ static void store(double* p, unsigned N, unsigned L, R, R r, R f) {
     reinterpret_cast<double2*>(p)[I * N + L] = make_double2(r, f - r);
@@ -88,6 +95,12 @@ struct Codec<float> {
     const float2 v = reinterpret_cast<const float2*>(p)[I * N + L];
     r = v.x;
     b = v.y;
+  }
+  template <int I>
+  __device__ __forceinline__ static void load_fr(const float* __restrict__ p, unsigned N, unsigned L, R, R& f, R& r) {
+    const float2 v = reinterpret_cast<const float2*>(p)[I * N + L];
+    r = v.x;
+    f = v.x + v.y;
   }
   template <int I>
   __device__ __forceinline__ static void store(float* p, unsigned N, unsigned L, R, R r, R f) {
@@ -111,6 +124,18 @@ struct Codec<__half> {
     const R f = fmaf(wr * (1.0f / 4096.0f), q, wr);
     r = f * c;
     b = f - r;
+  }
+  // the stored total f directly (and its red part): no b = f - r round trip
+  template <int I>
+  __device__ __forceinline__ static void load_fr(const __half* __restrict__ p, unsigned N, unsigned L, R rref, R& f,
+                                                 R& r) {
+    const unsigned w = reinterpret_cast<const unsigned*>(p)[I * N + L];
+    const R q = __half2float(__ushort_as_half((unsigned short)(w & 0xffffu)));
+    const R kf = __uint_as_float(0x4B000000u | (w >> 16));
+    const R c = fmaf(kf, 1.0f / 32768.0f, -(8388608.0f + 16384.0f) / 32768.0f);
+    const R wr = R(W(I)) * rref;
+    f = fmaf(wr * (1.0f / 4096.0f), q, wr);
+    r = f * c;
   }
   template <int I>
   __device__ __forceinline__ static void store(__half* p, unsigned N, unsigned L, R irref, R r, R f) {
@@ -425,18 +450,18 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
       for (int i = 0; i < 19; i++) asm volatile("prefetch.global.L2 [%0];" ::"l"(pin_ + 2 * (i * N + L + sx)));
     }
     // calmacros on the own populations
+    // (rho_B = rho - rho_R: a pure colour stays exactly pure, as r = f there)
     R f[19];
-    R sr = R(0), sb = R(0);
+    R sr = R(0), rho = R(0);
     const R rref = REF ? R(1) / R(rr_old[pd.idx(x, yc, zc)]) : R(P.rho0);
     unroll19([&](auto ic) {
       constexpr int i = decltype(ic)::value;
-      R r, b;
-      Codec<S>::template load<i>(pin_, N, L, rref, r, b);
-      f[i] = r + b;
+      R r;
+      Codec<S>::template load_fr<i>(pin_, N, L, rref, f[i], r);
       sr = sr + r;
-      sb = sb + b;
+      rho = rho + f[i];
     });
-    const R rho = sr + sb;
+    const R sb = rho - sr;
     R ux = R(0), uy = R(0), uz = R(0);
 #pragma unroll
     for (int i = 0; i < 19; i++) {
