@@ -1,9 +1,10 @@
 // batch.cu -- many independent CONFIG domains stepped together.
 //
 // One step of a batch is one CUDA graph:
-//   k_finalize_batch  calmacros of every domain in one launch, from the colour
-//                     densities the previous collide accumulated (blocks map
-//                     to domains through a prefix sum of per-domain block counts);
+//   phase field       calmacros of every domain in one launch (blocks map to
+//                     domains through a prefix sum of per-domain block
+//                     counts): from the colour densities the previous collide
+//                     accumulated (FP64) or from the populations (16-bit, FP32);
 //   sparse work       particle coupling and pin fill of every domain with
 //                     solids, one launch per subroutine for all of them
 //                     (sparse.cu);
@@ -55,6 +56,19 @@ struct TileEntry {
 constexpr int kTPB = BZ * BY;
 
 // blk[b] = (domain, block index within the domain) of phase block b
+template <typename S>
+__global__ void __launch_bounds__(256) k_phase_batch(const DomainDesc* __restrict__ descs,
+                                                     const int2* __restrict__ blk) {
+  using R = typename Codec<S>::R;
+  const int2 e = blk[blockIdx.x];
+  const DomainDesc& D = descs[e.x];
+  const long long L = (long long)e.y * 256 + threadIdx.x;
+  if (D.solid)
+    phase_node<S, true>(D.P, D.pd, (const S*)D.pin, (R*)D.phic, D.walls_all, D.rr_old, D.rr_new, L);
+  else
+    phase_node<S, false>(D.P, D.pd, (const S*)D.pin, (R*)D.phic, D.walls_all, D.rr_old, D.rr_new, L);
+}
+
 template <typename S>
 __global__ void __launch_bounds__(256) k_finalize_batch(const DomainDesc* __restrict__ descs,
                                                         const int2* __restrict__ blk) {
@@ -208,7 +222,10 @@ DomainDesc make_desc(sym_handle* h, int cur, int pc) {
 template <typename S>
 int enqueue_batch_step(sym_batch* b, int k, cudaEvent_t* ev) {
   if (ev) cudaEventRecord(ev[0], b->st);
-  k_finalize_batch<S><<<(unsigned)b->nblocks, 256, 0, b->st>>>(b->d_desc[k], b->d_blk);
+  if constexpr (kAccumulate<S>)
+    k_finalize_batch<S><<<(unsigned)b->nblocks, 256, 0, b->st>>>(b->d_desc[k], b->d_blk);
+  else
+    k_phase_batch<S><<<(unsigned)b->nblocks, 256, 0, b->st>>>(b->d_desc[k], b->d_blk);
   if (ev) cudaEventRecord(ev[1], b->st);
   if (int e = sparse_enqueue(b->sparse, k, b->st)) return berr(b, e, "sparse step");
   if (ev) cudaEventRecord(ev[2], b->st);

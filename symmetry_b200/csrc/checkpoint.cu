@@ -57,7 +57,7 @@ std::vector<Section> sections(sym_handle* h, bool fused) {
     s.push_back({"phase_field", F.storage == SYM_STORE_FP64 ? (void*)F.phi[1 - F.pc] : (void*)F.phif[1 - F.pc],
                  phib});
     if (F.storage == SYM_STORE_FP16) s.push_back({"ref_density", F.rref[1 - F.pc], sizeof(float) * pd.size()});
-    s.push_back({"accumulators", F.acc, 2 * N * (F.storage == SYM_STORE_FP64 ? 8 : 4)});
+    if (F.acc) s.push_back({"accumulators", F.acc, 2 * N * 8});
     s.push_back({"status", F.status, sizeof(int)});
     if (h->dp.par > 0) s.push_back({"ffi", h->ffi, 19 * ND});   // held from creation
   } else {

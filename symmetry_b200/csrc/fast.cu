@@ -85,14 +85,24 @@ int enqueue_step(sym_handle* h, int cur, int pc, cudaEvent_t* ev) {
   S* pnext = popbuf<S>(h, 1 - cur);
   R* phic = phibuf<S>(h, pc);
   R* phip = phibuf<S>(h, 1 - pc);
-  // (a1) calmacros from the colour densities the previous collide accumulated
+  // (a1) calmacros: from the colour densities the previous collide
+  // accumulated, or from the populations
   if (ev) cudaEventRecord(ev[0], h->st);
-  if (solid)
-    k_finalize<S, true><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, accbuf<S>(h), phic, h->walls_all, rr_new(h, pc),
-                                                            h->fast.status);
-  else
-    k_finalize<S, false><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, accbuf<S>(h), phic, h->walls_all, rr_new(h, pc),
-                                                             h->fast.status);
+  if constexpr (kAccumulate<S>) {
+    if (solid)
+      k_finalize<S, true><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, accbuf<S>(h), phic, h->walls_all, rr_new(h, pc),
+                                                              h->fast.status);
+    else
+      k_finalize<S, false><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, accbuf<S>(h), phic, h->walls_all,
+                                                               rr_new(h, pc), h->fast.status);
+  } else {
+    if (solid)
+      k_phase<S, true><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, pin_, phic, h->walls_all, rr_old(h, pc),
+                                                           rr_new(h, pc));
+    else
+      k_phase<S, false><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, pin_, phic, h->walls_all, rr_old(h, pc),
+                                                            rr_new(h, pc));
+  }
   if (ev) cudaEventRecord(ev[1], h->st);
   // particle coupling and pin fill (cur and pc advance together from 0)
   if (int e = sparse_enqueue(h->fast.sparse, cur, h->st)) return set_error(h, e, "sparse step");
@@ -181,7 +191,8 @@ int fast_alloc(sym_handle* h) {
     if (F.storage == SYM_STORE_FP16)
       if (int e = dev_carve(h, (void**)&F.rref[k], sizeof(float) * pd.size())) return e;
   }
-  if (int e = dev_carve(h, &F.acc, 2 * h->N * (F.storage == SYM_STORE_FP64 ? 8 : 4))) return e;
+  if (F.storage == SYM_STORE_FP64)   // the storage whose collide kernel accumulates (kAccumulate)
+    if (int e = dev_carve(h, &F.acc, 2 * h->N * 8)) return e;
   if (int e = dev_carve(h, (void**)&F.status, sizeof(int))) return e;
   if (h->planning) return SYM_OK;
   F.bytes = h->bytes - before;

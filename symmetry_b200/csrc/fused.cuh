@@ -177,6 +177,15 @@ struct Acc<float> {
   __device__ __forceinline__ static float val(T a) { return (float)(int)a * 0x1p-26f; }
   __device__ __forceinline__ static bool ok(float v) { return fabsf(v) < 31.0f; }
 };
+// Whether the collide kernel of storage S accumulates the next step's colour
+// densities (the phase field then reads 2 values per node) or the phase field
+// re-reads the populations (38 per node).  The accumulation costs arithmetic
+// (warp shuffles, a shared-memory exchange, atomics), the re-read costs
+// bytes: FP64 storage, bound by memory, accumulates; the 16-bit and FP32
+// storages, bound by instruction issue, re-read.
+template <typename S>
+constexpr bool kAccumulate = sizeof(S) == 8;
+
 // add v to accumulator p (a reduction: nothing is returned); out-of-range
 // values set *status and add nothing
 template <typename R>
@@ -198,6 +207,46 @@ __device__ __forceinline__ void unroll19(F&& f) {
 }
 
 // ---- calmacros (Source1.f90:770-831) on the fused state ---------------------------
+// Storages that do not accumulate: phi = (rhoR - rhoB) / rho from the node's
+// own post-stream populations; 0 on solid nodes.  16-bit storage decodes with
+// rr_old and records 1/rho in rr_new (as finalize_node below).
+template <typename S, bool SOLID>
+__device__ __forceinline__ void phase_node(const DevParams& P, const Pad& pd, const S* __restrict__ pops,
+                                           typename Codec<S>::R* __restrict__ phi,
+                                           const int32_t* __restrict__ walls_all, const float* __restrict__ rr_old,
+                                           float* __restrict__ rr_new, long long L) {
+  using R = typename Codec<S>::R;
+  if (L >= P.N) return;
+  const unsigned Lu = (unsigned)L, q = Lu / (unsigned)P.nz;
+  const int z = (int)(Lu - q * (unsigned)P.nz), x = (int)(q / (unsigned)P.ny), y = (int)(q - (unsigned)x * P.ny);
+  R v = R(0);
+  R rho = R(P.rho0);
+  if (!(SOLID && walls_all[L] >= 1)) {
+    const unsigned N = (unsigned)P.N;
+    const R rref = Codec<S>::kRef ? R(1) / R(rr_old[pd.idx(x, y, z)]) : R(P.rho0);
+    R sr = R(0), sf = R(0);
+    unroll19([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      R f, r;
+      Codec<S>::template load_fr<i>(pops, N, Lu, rref, f, r);
+      sr = sr + r;
+      sf = sf + f;
+    });
+    rho = sf;
+    v = qdiv<R>(sr - (sf - sr), rho);
+  }
+  phi_store<R>(P, pd, phi, x, y, z, v);
+  if (Codec<S>::kRef) phi_store<float>(P, pd, rr_new, x, y, z, 1.0f / float(rho));
+}
+
+template <typename S, bool SOLID>
+__global__ void __launch_bounds__(256) k_phase(DevParams P, Pad pd, const S* __restrict__ pops,
+                                               typename Codec<S>::R* __restrict__ phi,
+                                               const int32_t* __restrict__ walls_all, const float* __restrict__ rr_old,
+                                               float* __restrict__ rr_new) {
+  phase_node<S, SOLID>(P, pd, pops, phi, walls_all, rr_old, rr_new, blockIdx.x * 256LL + threadIdx.x);
+}
+
 // From the accumulated colour densities (the steady-state phase field):
 // phi = (rhoR - rhoB) / rho on fluid nodes, 0 on solid nodes, written with its
 // periodic ghost images; the accumulators are cleared for the collide kernel
@@ -325,6 +374,7 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
   // solid handling: compiled in (SOLID) and wanted by this domain (solid_rt);
   // the batched kernel compiles one variant and decides per tile
   const bool SOLIDX = SOLID && solid_rt;
+  constexpr bool ACC = kAccumulate<S>;
   constexpr bool REF = Codec<S>::kRef;
   const int tz = threadIdx.x % BZ, ty = threadIdx.x / BZ;
   const unsigned N = (unsigned)P.N;
@@ -443,7 +493,9 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
 #pragma unroll
         for (int c = 0; c < 2; c++) g[a][b][c] = R(0);
     R sfr = R(0), sfb = R(0);
-    if (__any_sync(0xffffffffu, act)) {
+    // accumulating kernels run every lane of a warp with an active node (the
+    // shuffles need the whole warp); the others skip inactive nodes
+    if (ACC ? __any_sync(0xffffffffu, act) : act) {
     if (x + 1 < xb) {
       // bring the next plane's populations toward L2 while this plane computes
 #pragma unroll
@@ -572,6 +624,7 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
         const R irr =
             REF ? R(sm.irr[(x + CX(i) + kIrrRing) % kIrrRing][(ty + 2 + CY(i)) * (BZ + 4) + tz + 2 + CZ(i)]) : irho0;
         Codec<S>::template store<i>(pout_, N, T, irr, r, f[i]);
+        if constexpr (!ACC) return;
         const R bv = f[i] - r;
         const bool ext = (CX(i) > 0 && exp_) || (CX(i) < 0 && exm) || (CY(i) > 0 && eyp) || (CY(i) < 0 && eym) ||
                          (CZ(i) > 0 && ezp) || (CZ(i) < 0 && ezm);
@@ -589,7 +642,7 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
           zm[1] = bv;
         }
       }();
-      if constexpr (CZ(i) < 0) {
+      if constexpr (ACC && CZ(i) < 0) {
         // last of a group with cz = 0, +1, -1: lane l receives the cz = +1 push
         // of lane l-1 and the cz = -1 push of lane l+1 (lane = tz)
 #pragma unroll
@@ -603,39 +656,41 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
       }
     });
     }
-    // along y through shared memory: row ty+1 receives the cy = +1 sums of row
-    // ty and row ty-1 the cy = -1 sums, for each destination plane
+    if constexpr (ACC) {
+      // along y through shared memory: row ty+1 receives the cy = +1 sums of row
+      // ty and row ty-1 the cy = -1 sums, for each destination plane
 #pragma unroll
-    for (int a = 0; a < 3; a++)
+      for (int a = 0; a < 3; a++)
 #pragma unroll
-      for (int c = 0; c < 2; c++) {
-        sm.xch[a][0][c][ty][tz] = g[a][2][c];
-        sm.xch[a][1][c][ty][tz] = g[a][0][c];
+        for (int c = 0; c < 2; c++) {
+          sm.xch[a][0][c][ty][tz] = g[a][2][c];
+          sm.xch[a][1][c][ty][tz] = g[a][0][c];
+        }
+      __syncthreads();
+      R in[3][2];
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int c = 0; c < 2; c++) {
+          R v = g[a][1][c];
+          if (ty > 0) v = v + sm.xch[a][0][c][ty - 1][tz];
+          if (ty < BY - 1) v = v + sm.xch[a][1][c][ty + 1][tz];
+          in[a][c] = v;
+        }
+      aPr = aPr + in[0][0]; aPb = aPb + in[0][1];
+      aCr = aCr + in[1][0] + sfr; aCb = aCb + in[1][1] + sfb;
+      aNr = aNr + in[2][0]; aNb = aNb + in[2][1];
+      // plane x-1 of this column has all its in-tile contributions
+      if (x > xa && inr && (aPr != R(0) || aPb != R(0))) {
+        acc_add<R>(accR + (L - sx), aPr, status);
+        acc_add<R>(accB + (L - sx), aPb, status);
       }
-    __syncthreads();
-    R in[3][2];
-#pragma unroll
-    for (int a = 0; a < 3; a++)
-#pragma unroll
-      for (int c = 0; c < 2; c++) {
-        R v = g[a][1][c];
-        if (ty > 0) v = v + sm.xch[a][0][c][ty - 1][tz];
-        if (ty < BY - 1) v = v + sm.xch[a][1][c][ty + 1][tz];
-        in[a][c] = v;
-      }
-    aPr = aPr + in[0][0]; aPb = aPb + in[0][1];
-    aCr = aCr + in[1][0] + sfr; aCb = aCb + in[1][1] + sfb;
-    aNr = aNr + in[2][0]; aNb = aNb + in[2][1];
-    // plane x-1 of this column has all its in-tile contributions
-    if (x > xa && inr && (aPr != R(0) || aPb != R(0))) {
-      acc_add<R>(accR + (L - sx), aPr, status);
-      acc_add<R>(accB + (L - sx), aPb, status);
+      aPr = aCr; aPb = aCb;
+      aCr = aNr; aCb = aNb;
+      aNr = R(0); aNb = R(0);
     }
-    aPr = aCr; aPb = aCb;
-    aCr = aNr; aCb = aNb;
-    aNr = R(0); aNb = R(0);
   }
-  if (xb > xa && inr && (aPr != R(0) || aPb != R(0))) {
+  if (ACC && xb > xa && inr && (aPr != R(0) || aPb != R(0))) {
     const unsigned L = (unsigned)(z + sy * y + sx * (xb - 1));
     acc_add<R>(accR + L, aPr, status);
     acc_add<R>(accB + L, aPb, status);
@@ -794,11 +849,14 @@ __global__ void k_import_pops(DevParams P, Pad pd, const double* __restrict__ ri
     sr = sr + r;
     sb = sb + b;
   });
-  // the accumulators the first phase field after the import reads
+  // the accumulators the first phase field after the import reads (storages
+  // that accumulate)
   using A = Acc<R>;
-  if (!A::ok(sr) || !A::ok(sb)) atomicOr(status, 1);
-  acc[L] = A::ok(sr) ? A::fix(sr) : 0;
-  acc[L + P.N] = A::ok(sb) ? A::fix(sb) : 0;
+  if (acc) {
+    if (!A::ok(sr) || !A::ok(sb)) atomicOr(status, 1);
+    acc[L] = A::ok(sr) ? A::fix(sr) : 0;
+    acc[L + P.N] = A::ok(sb) ? A::fix(sb) : 0;
+  }
 }
 template <typename S>
 __global__ void k_export_pops(DevParams P, Pad pd, const S* __restrict__ pops, const float* __restrict__ rr, double* ri,

@@ -288,7 +288,7 @@ __global__ void __launch_bounds__(kT) k_sp_curve2(const SpDom* __restrict__ doms
     db += vb - (double)hb;
   });
   using AT = typename Acc<R>::T;
-  if (dr != 0.0 || db != 0.0) {
+  if (kAccumulate<S> && (dr != 0.0 || db != 0.0)) {
     acc_add<R>((AT*)D.acc + L, R(dr), D.status);
     acc_add<R>((AT*)D.acc + P.N + L, R(db), D.status);
   }
