@@ -140,8 +140,8 @@ def test_c2_walls_particle_300_steps():
     compare_particles(o, L, 1, 1e-9, ["center", "up", "rp"])
 
 
-def test_reference_mode_20_steps():
-    """The reference's own geometry (mirrors, x=1/z=1 walls, 12 particles), 48x88x48."""
+def test_reference_mode_200_steps():
+    """The reference's own geometry (mirrors, x=1/z=1 walls, 12 particles), 48x88x48, 200 steps."""
     p = params.reference_params(48, 88, 48)
     o = setup_reference(p)
     L = Lattice(p)
@@ -152,8 +152,8 @@ def test_reference_mode_20_steps():
     compare_masks(o, L)
     compare_particles(o, L, 12, 1e-13, ["center", "center0"])
     compare_fields(o, L, ["rho_N", "rho", "ri", "bi"], 1e-13)
-    o.step(20)
-    L.step(20)
+    o.step(200)
+    L.step(200)
     for f in ["rho", "ux", "uy", "uz", "rho_N"]:
         e = rel_l2(L.get(f), o.arr(f))
         assert e <= 1e-10, (f, e)

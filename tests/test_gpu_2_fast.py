@@ -92,10 +92,10 @@ def test_fast_fp64_c2_interpolated_bounce_back_300_steps():
     compare_particles(o, L, 1, 1e-9, ["center", "up", "rp"])
 
 
-def test_fast_fp64_c2_full_size_100_steps():
-    """configs[1] at its full 64x64x128 size (short run)."""
+def test_fast_fp64_c2_full_size_1000_steps():
+    """The wetting-wall slab with one moving sphere at its full 64x64x128 size."""
     w = configs.c2_wall_particle()
-    o, L = fast_run(w, 100)
+    o, L = fast_run(w, 1000)
     fluid = o.arr("walls_all") == 0
     e = errors(o, L, mask=fluid)
     assert max(e.values()) <= 1e-10, e
