@@ -41,6 +41,7 @@ extern "C" {
 #define SYM_ERR_STATE       6  /* call not valid in the current state                */
 #define SYM_ERR_UNSUPPORTED 7  /* feature not available for this mode/storage        */
 #define SYM_ERR_NOTFOUND    8  /* unknown field / job id                             */
+#define SYM_ERR_DRIFT       9  /* a served job's conserved quantity drifted          */
 
 /* ---- geometry modes ---------------------------------------------------- */
 /* REFERENCE: the reference's own domain (Source1.f90:4, 1443-1592): updates on
@@ -282,6 +283,14 @@ typedef struct sym_job_spec {
   double center[3];     /* particle centre (p.par == 1)                          */
   double up[3];         /* particle velocity                                     */
   double t_arrival;     /* arrival on the server clock in seconds; < 0 = now     */
+  /* failure detection (no counterpart in the reference, which only warns):
+   * drift_tol     > 0: FAILED with SYM_ERR_DRIFT when the red-phase volume
+   *               sum (1+phi)/2 moves by more than drift_tol (relative) from
+   *               the admission reading (evaporation or a blow-up);
+   * wall_budget_s > 0: FAILED with SYM_ERR_TIMEOUT when the job has been
+   *               resident longer than this many seconds at a check.       */
+  double drift_tol;
+  double wall_budget_s;
 } sym_job_spec;
 
 typedef struct sym_job_result {

@@ -48,6 +48,7 @@ struct Job {
   double r_prev = 0.0;    // min r_eq at the previous check
   int slot = -1;          // row of the pinned plane-sum buffer
   bool checking = false;  // a reading was enqueued this round
+  double vol0 = 0.0;      // red-phase volume at admission (failure detection)
 };
 
 double stop_radius(const sym_job_spec& s) { return s.stop_radius > 0 ? s.stop_radius : 1.0; }
@@ -129,6 +130,14 @@ int ensure_rows(sym_server* s, int len) {
   return SYM_OK;
 }
 
+// red-phase volume: the sum of the per-plane red areas of a job's pinned row
+double vol_of(const sym_server* s, const Job& j) {
+  const double* a = s->hplanes + (size_t)j.slot * s->row_len;
+  double v = 0.0;
+  for (int z = 0; z < j.spec.p.nz; z++) v += a[z];
+  return v;
+}
+
 // min over z of sqrt(area/pi) from a job's pinned row
 double rmin_of(const sym_server* s, const Job& j) {
   const double* a = s->hplanes + (size_t)j.slot * s->row_len;
@@ -151,6 +160,7 @@ int first_reading(sym_server* s, Job& j) {
   j.r_prev = rmin_of(s, j);
   j.s_prev = 0;
   j.r.rmin = j.r_prev;
+  j.vol0 = vol_of(s, j);
   return SYM_OK;
 }
 
@@ -367,8 +377,15 @@ int sym_server_tick(sym_server* s, int max_steps, int* running, int* pending) {
         const double r = rmin_of(s, j);
         j.r.rmin = r;
         const double thr = stop_radius(j.spec);
+        const double dv = j.vol0 > 0.0 ? std::fabs(vol_of(s, j) - j.vol0) / j.vol0 : 0.0;
         if (!(r == r)) {
           finish(s, j, SYM_JOB_FAILED, SYM_ERR_NAN);
+          end = true;
+        } else if (j.spec.drift_tol > 0.0 && dv > j.spec.drift_tol) {
+          finish(s, j, SYM_JOB_FAILED, SYM_ERR_DRIFT);
+          end = true;
+        } else if (j.spec.wall_budget_s > 0.0 && now(s) - j.r.t_admit > j.spec.wall_budget_s) {
+          finish(s, j, SYM_JOB_FAILED, SYM_ERR_TIMEOUT);
           end = true;
         } else if (r < thr) {
           const double f = (j.r_prev > r) ? (j.r_prev - thr) / (j.r_prev - r) : 1.0;

@@ -364,7 +364,8 @@ class Batch:
             pass
 
 
-def job_spec(w, max_steps: int, stop_radius: float = 1.0, t_arrival: float = -1.0) -> SymJobSpec:
+def job_spec(w, max_steps: int, stop_radius: float = 1.0, t_arrival: float = -1.0, drift_tol: float = 0.0,
+             wall_budget_s: float = 0.0) -> SymJobSpec:
     """The sym_job_spec of a workload (same initial state as setup_workload)."""
     js = SymJobSpec()
     js.p = w.params.copy()
@@ -386,6 +387,8 @@ def job_spec(w, max_steps: int, stop_radius: float = 1.0, t_arrival: float = -1.
             js.center[k] = float(q["center"][k])
             js.up[k] = float(q.get("up", [0.0, 0.0, 0.0])[k])
     js.t_arrival = float(t_arrival)
+    js.drift_tol = float(drift_tol)
+    js.wall_budget_s = float(wall_budget_s)
     return js
 
 

@@ -152,6 +152,7 @@ class SymJobSpec(ctypes.Structure):
         ("stop_radius", ctypes.c_double),
         ("center", ctypes.c_double * 3), ("up", ctypes.c_double * 3),
         ("t_arrival", ctypes.c_double),
+        ("drift_tol", ctypes.c_double), ("wall_budget_s", ctypes.c_double),
     ]
 
 

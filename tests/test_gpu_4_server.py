@@ -157,3 +157,21 @@ def test_unstable_job_fails_with_nan():
     assert 100 <= r.steps <= 300
     assert q.status == 3 and math.isfinite(q.rmin)
     S.close()
+
+
+def test_drift_and_wall_budget_retire_jobs():
+    """Failure detection beyond non-finite readings: a red-volume drift over the
+    job's tolerance retires it with SYM_ERR_DRIFT, a resident time over its
+    wall budget with SYM_ERR_TIMEOUT; a job without limits runs to its step cap
+    beside them."""
+    w = configs.c1_thread(nx=20, ny=20, nz=48, radius=4.0)
+    S = Server(slots=4, check_every=10)
+    a = S.submit(job_spec(w, 60, drift_tol=1e-14))
+    b = S.submit(job_spec(w, 60, wall_budget_s=1e-9))
+    c = S.submit(job_spec(w, 60))
+    S.run_until_idle()
+    ra, rb, rc = S.result(a), S.result(b), S.result(c)
+    S.close()
+    assert ra.status == 4 and ra.error == 9, ra.as_dict()
+    assert rb.status == 4 and rb.error == 5, rb.as_dict()
+    assert rc.status == 3 and rc.steps == 60, rc.as_dict()
