@@ -10,8 +10,8 @@ from symmetry_b200.params import SymJobResult, SymJobSpec, SymParams
 
 
 def test_job_struct_layout():
-    # sym_job_spec: sym_params + 2 int32 + 5 doubles + uint64 + 8 doubles
-    assert ctypes.sizeof(SymJobSpec) == ctypes.sizeof(SymParams) + 2 * 4 + 5 * 8 + 8 + 8 * 8
+    # sym_job_spec: sym_params + 2 int32 + 5 doubles + uint64 + 10 doubles
+    assert ctypes.sizeof(SymJobSpec) == ctypes.sizeof(SymParams) + 2 * 4 + 5 * 8 + 8 + 10 * 8
     # sym_job_result: 4 int32 + 5 doubles + int64
     assert ctypes.sizeof(SymJobResult) == 4 * 4 + 5 * 8 + 8
 
