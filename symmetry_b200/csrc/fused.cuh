@@ -327,7 +327,9 @@ struct Smem {
   alignas(128) R phi[5][kPhiSlot];
   alignas(128) float irr[Codec<S>::kRef ? kIrrRing : 1][kIrrSlot];   // 1/rho_ref of this step (16-bit storage)
   NormalV<R> n[4][BY + 2][BZ + 2];   // [plane][y][z]: n and |grad phi|
-  R xch[3][2][2][BY][BZ];   // [cx+1][to row y+1, y-1][colour]: density sums crossing rows
+  // [plane parity][cx+1][to row y+1, y-1][colour]: density sums crossing rows
+  // (accumulating storages; written at one plane, read after the next plane's barrier)
+  R xch[kAccumulate<S> ? 2 : 1][3][2][2][BY][BZ];
   uint64_t bar[kIrrRing];   // one mbarrier per plane load, used round robin
 };
 // dynamic shared memory of the collide kernels: the Smem block on a 128-byte
@@ -466,7 +468,37 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
   using AT = typename Acc<R>::T;
   AT* const accR = acc;
   AT* const accB = acc + N;
-  R aPr = R(0), aPb = R(0), aCr = R(0), aCb = R(0), aNr = R(0), aNb = R(0);   // planes x-1, x, x+1
+  R aPr = R(0), aPb = R(0), aCr = R(0), aCb = R(0), aNr = R(0), aNb = R(0);   // planes k-1, k, k+1
+  R gk[3][2];   // this column's own sums of plane k (cy = 0, bounce-backs), kept for the combine
+  // Combine the in-tile sums computed at plane k -- own sums gk plus the
+  // cy = +-1 sums the neighbouring rows left in xch[k & 1] -- into the planes
+  // k-1, k, k+1 of this column; plane k-1 then has all its in-tile
+  // contributions and is added to the accumulators.  Runs after the barrier
+  // that follows plane k's writes (the next plane's, or the final one).
+  auto combine = [&](int k) {
+    const int q = k & 1;
+    R in[3][2];
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        R v = gk[a][c];
+        if (ty > 0) v = v + sm.xch[q][a][0][c][ty - 1][tz];
+        if (ty < BY - 1) v = v + sm.xch[q][a][1][c][ty + 1][tz];
+        in[a][c] = v;
+      }
+    aPr = aPr + in[0][0]; aPb = aPb + in[0][1];
+    aCr = aCr + in[1][0]; aCb = aCb + in[1][1];
+    aNr = aNr + in[2][0]; aNb = aNb + in[2][1];
+    if (k > xa && inr && (aPr != R(0) || aPb != R(0))) {
+      const unsigned Lp = (unsigned)(z + sy * y + sx * (k - 1));
+      acc_add<R>(accR + Lp, aPr, status);
+      acc_add<R>(accB + Lp, aPb, status);
+    }
+    aPr = aCr; aPb = aCb;
+    aCr = aNr; aCb = aNb;
+    aNr = R(0); aNb = R(0);
+  };
   for (int x = xa; x < xb; x++) {
     // phi of plane x+3 on its way; normals of plane x+1 from phi planes x..x+2.
     // The slots the load overwrites (phi of plane x-2, 1/rho_ref of plane x-3)
@@ -475,6 +507,9 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
     wait_phi(x + 2);
     compute_n(x + 1);
     __syncthreads();
+    if constexpr (ACC) {
+      if (x > xa) combine(x - 1);
+    }
     const unsigned L = (unsigned)(zc + sy * yc + sx * x);
     int pp = 0;
     bool act = inr;
@@ -657,37 +692,26 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
     });
     }
     if constexpr (ACC) {
-      // along y through shared memory: row ty+1 receives the cy = +1 sums of row
-      // ty and row ty-1 the cy = -1 sums, for each destination plane
+      // along y through shared memory: row ty+1 takes the cy = +1 sums of row
+      // ty and row ty-1 the cy = -1 sums, for each destination plane (read in
+      // the combine after the next barrier)
+      const int q = x & 1;
 #pragma unroll
       for (int a = 0; a < 3; a++)
 #pragma unroll
         for (int c = 0; c < 2; c++) {
-          sm.xch[a][0][c][ty][tz] = g[a][2][c];
-          sm.xch[a][1][c][ty][tz] = g[a][0][c];
+          sm.xch[q][a][0][c][ty][tz] = g[a][2][c];
+          sm.xch[q][a][1][c][ty][tz] = g[a][0][c];
+          gk[a][c] = g[a][1][c];
         }
+      gk[1][0] = gk[1][0] + sfr;
+      gk[1][1] = gk[1][1] + sfb;
+    }
+  }
+  if constexpr (ACC) {
+    if (xb > xa) {
       __syncthreads();
-      R in[3][2];
-#pragma unroll
-      for (int a = 0; a < 3; a++)
-#pragma unroll
-        for (int c = 0; c < 2; c++) {
-          R v = g[a][1][c];
-          if (ty > 0) v = v + sm.xch[a][0][c][ty - 1][tz];
-          if (ty < BY - 1) v = v + sm.xch[a][1][c][ty + 1][tz];
-          in[a][c] = v;
-        }
-      aPr = aPr + in[0][0]; aPb = aPb + in[0][1];
-      aCr = aCr + in[1][0] + sfr; aCb = aCb + in[1][1] + sfb;
-      aNr = aNr + in[2][0]; aNb = aNb + in[2][1];
-      // plane x-1 of this column has all its in-tile contributions
-      if (x > xa && inr && (aPr != R(0) || aPb != R(0))) {
-        acc_add<R>(accR + (L - sx), aPr, status);
-        acc_add<R>(accB + (L - sx), aPb, status);
-      }
-      aPr = aCr; aPb = aCb;
-      aCr = aNr; aCb = aNb;
-      aNr = R(0); aNb = R(0);
+      combine(xb - 1);
     }
   }
   if (ACC && xb > xa && inr && (aPr != R(0) || aPb != R(0))) {
