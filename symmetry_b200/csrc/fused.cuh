@@ -329,7 +329,7 @@ struct Smem {
   NormalV<R> n[4][BY + 2][BZ + 2];   // [plane][y][z]: n and |grad phi|
   // [plane parity][cx+1][to row y+1, y-1][colour]: density sums crossing rows
   // (accumulating storages; written at one plane, read after the next plane's barrier)
-  R xch[kAccumulate<S> ? 2 : 1][3][2][2][BY][BZ];
+  R xch[kAccumulate<S> ? 2 : 1][kAccumulate<S> ? 3 : 1][2][2][kAccumulate<S> ? BY : 1][kAccumulate<S> ? BZ : 1];
   uint64_t bar[kIrrRing];   // one mbarrier per plane load, used round robin
 };
 // dynamic shared memory of the collide kernels: the Smem block on a 128-byte
