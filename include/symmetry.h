@@ -159,6 +159,27 @@ int sym_set_populations(sym_handle* h, const double* ri, const double* bi);
  * stays authoritative, so reading does not re-encode reduced storage.  Any
  * pointer may be NULL. */
 int sym_get_macros(sym_handle* h, double* rho, double* ux, double* uy, double* uz, double* rho_n);
+
+/* Error flags the fused kernels recorded on the device since the fused state
+ * was last built from the canonical one (no counterpart in the reference):
+ *   SYM_DEV_NONFINITE  FP64 storage: a next-step colour density was not
+ *                      finite or left the fixed-point accumulator's range
+ *   SYM_DEV_TIMEOUT    a tile load did not complete within the bounded wait
+ *                      (the kernel carried on instead of hanging)
+ * In FP64 storage either flag also makes every later phase field NaN.  The
+ * server reads the flags of a job at each of its checks and retires it as
+ * failed (SYM_ERR_TIMEOUT, SYM_ERR_NAN).  0 when nothing was recorded or the
+ * handle never ran the fused path. */
+#define SYM_DEV_NONFINITE 1
+#define SYM_DEV_TIMEOUT   2
+int sym_device_status(sym_handle* h, int32_t* flags);
+
+/* Runs the timeout path of the bounded mbarrier wait the fused kernels use
+ * for their tile loads: one thread waits `polls` polls on a barrier that
+ * nothing arrives on.  *status receives the flags the kernels would record
+ * (SYM_DEV_TIMEOUT; bit 4 if a completed barrier was not seen), *ms the
+ * event-timed duration of the launch.  Allocates 4 bytes of device memory. */
+int sym_selftest_wait_timeout(int device, int polls, int32_t* status, double* ms, char* msg, size_t msg_len);
 int sym_set_particles(sym_handle* h, const sym_particles* s);
 int sym_get_particles(sym_handle* h, sym_particles* s);
 /* Lagrange point arrays (par, La_num) column-major as in :1805; any pointer may be NULL. */
@@ -258,8 +279,9 @@ int sym_batch_kernels_per_step(sym_batch* b, int* kernels);
  * server reduces its phase field to r_eq(z) = sqrt(sum_xy (1+phi)/2 / pi) and
  * retires the job when min_z r_eq falls below its stop radius (breakup, time
  * interpolated linearly between the last two checks), when it reaches its
- * step limit, or when the field is no longer finite (failed, SYM_ERR_NAN).
- * Jobs are admitted only at multiples of `check_every` server steps, so a
+ * step limit, or as failed when the field is no longer finite (SYM_ERR_NAN)
+ * or the device recorded a timed-out tile load (SYM_ERR_TIMEOUT; see
+ * sym_device_status).  Jobs are admitted only at multiples of `check_every` server steps, so a
  * job's checks fall on the same steps whatever else runs beside it: its
  * result is the one it gets alone.  One host thread drives a server through
  * sym_server_tick. */

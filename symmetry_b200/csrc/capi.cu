@@ -643,5 +643,16 @@ int sym_mass_momentum(sym_handle* h, double out[5]) {
   if (int e = canonical(h)) return e;
   return ref_mass_momentum(h, out);
 }
+int sym_device_status(sym_handle* h, int32_t* flags) {
+  if (int e = guard(h)) return e;
+  if (!flags) return set_error(h, SYM_ERR_PARAM, "null output");
+  int32_t v = 0;
+  if (h->fast.status) {
+    cudaMemcpyAsync(&v, h->fast.status, sizeof(int32_t), cudaMemcpyDeviceToHost, h->st);
+    if (int e = check_cuda(h, cudaStreamSynchronize(h->st), "device status")) return e;
+  }
+  *flags = v;
+  return SYM_OK;
+}
 
 }  // extern "C"

@@ -74,6 +74,7 @@ struct sym_server {
   // pinned host rows for the per-plane reductions, one row per slot
   double* hplanes = nullptr;
   int row_len = 0;
+  int32_t* hflags = nullptr;    // pinned: each slot's device error flags at its last check
   std::vector<int> free_rows;
   cudaEvent_t ev[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
   double node_updates = 0.0;
@@ -117,6 +118,13 @@ void release(sym_server* s, Job& j) {
 
 // grow the pinned rows to `len` doubles (only between rounds: nothing in flight)
 int ensure_rows(sym_server* s, int len) {
+  if (!s->hflags) {
+    if (cudaMallocHost(&s->hflags, sizeof(int32_t) * (size_t)s->slots) != cudaSuccess) {
+      (void)cudaGetLastError();
+      s->hflags = nullptr;
+      return serr(s, SYM_ERR_OOM, "pinned host flags");
+    }
+  }
   if (len <= s->row_len && s->hplanes) return SYM_OK;
   const int nl = std::max(len, s->row_len);
   double* p = nullptr;
@@ -290,6 +298,7 @@ int sym_server_destroy(sym_server* s) {
   for (auto& kv : s->jobs)
     if (kv.second.h) sym_destroy(kv.second.h);
   if (s->hplanes) cudaFreeHost(s->hplanes);
+  if (s->hflags) cudaFreeHost(s->hflags);
   for (int m = 0; m < 3; m++)
     for (int k = 0; k < 2; k++)
       if (s->ev[m][k]) cudaEventDestroy(s->ev[m][k]);
@@ -359,6 +368,7 @@ int sym_server_tick(sym_server* s, int max_steps, int* running, int* pending) {
       if (int e = fast_neck_planes(j.h, j.h->red, st)) return serr(s, e, j.h->err);
       cudaMemcpyAsync(s->hplanes + (size_t)j.slot * s->row_len, j.h->red, sizeof(double) * j.spec.p.nz,
                       cudaMemcpyDeviceToHost, st);
+      cudaMemcpyAsync(s->hflags + j.slot, j.h->fast.status, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
     }
     for (int m = 0; m < 3; m++) {
       if (!s->batch[m]) continue;
@@ -378,7 +388,11 @@ int sym_server_tick(sym_server* s, int max_steps, int* running, int* pending) {
         j.r.rmin = r;
         const double thr = stop_radius(j.spec);
         const double dv = j.vol0 > 0.0 ? std::fabs(vol_of(s, j) - j.vol0) / j.vol0 : 0.0;
-        if (!(r == r)) {
+        const int32_t flags = s->hflags[j.slot];
+        if (flags & SYM_DEV_TIMEOUT) {
+          finish(s, j, SYM_JOB_FAILED, SYM_ERR_TIMEOUT);
+          end = true;
+        } else if (!(r == r) || (flags & SYM_DEV_NONFINITE)) {
           finish(s, j, SYM_JOB_FAILED, SYM_ERR_NAN);
           end = true;
         } else if (j.spec.drift_tol > 0.0 && dv > j.spec.drift_tol) {

@@ -48,9 +48,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return done != 0;
 }
 
-// bounded wait for the phase with the given parity; false after kSpinLimit polls
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (int it = 0; it < kSpinLimit; ++it)
+// bounded wait for the phase with the given parity; false after `limit` polls
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int limit = kSpinLimit) {
+  for (int it = 0; it < limit; ++it)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }

@@ -84,6 +84,9 @@ def lib() -> ctypes.CDLL:
         L.sym_output3.argtypes = [H, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int32)]
         L.sym_neck_radius.argtypes = [H, ctypes.POINTER(ctypes.c_double)]
         L.sym_mass_momentum.argtypes = [H, ctypes.c_void_p]
+        L.sym_device_status.argtypes = [H, ctypes.POINTER(ctypes.c_int32)]
+        L.sym_selftest_wait_timeout.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int32),
+                                                ctypes.POINTER(ctypes.c_double), ctypes.c_char_p, ctypes.c_size_t]
         L.sym_batch_create.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
         L.sym_batch_destroy.argtypes = [ctypes.c_void_p]
         L.sym_batch_last_error.restype = ctypes.c_char_p
@@ -118,6 +121,22 @@ def params_check(p: SymParams) -> Optional[str]:
     buf = ctypes.create_string_buffer(256)
     rc = lib().sym_params_check(ctypes.byref(p), buf, 256)
     return None if rc == 0 else buf.value.decode()
+
+
+DEV_NONFINITE = 1   # sym_device_status flags (include/symmetry.h)
+DEV_TIMEOUT = 2
+
+
+def selftest_wait_timeout(polls: int, device: int = 0):
+    """Run the timeout path of the fused kernels' bounded mbarrier wait:
+    returns (flags, ms) -- the flags a timed-out tile load records and the
+    event-timed duration of the launch."""
+    st, ms = ctypes.c_int32(), ctypes.c_double()
+    buf = ctypes.create_string_buffer(256)
+    rc = lib().sym_selftest_wait_timeout(device, polls, ctypes.byref(st), ctypes.byref(ms), buf, 256)
+    if rc:
+        raise SymError(rc, "selftest_wait_timeout: " + buf.value.decode())
+    return st.value, ms.value
 
 
 def footprint(p: SymParams) -> int:
@@ -298,6 +317,12 @@ class Lattice:
         out = np.zeros(5)
         self._ck(lib().sym_mass_momentum(self.h, out.ctypes.data), "mass_momentum")
         return out
+
+    def device_status(self) -> int:
+        """Error flags the fused kernels recorded (DEV_NONFINITE | DEV_TIMEOUT)."""
+        v = ctypes.c_int32()
+        self._ck(lib().sym_device_status(self.h, ctypes.byref(v)), "device_status")
+        return v.value
 
 
 class Batch:

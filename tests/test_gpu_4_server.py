@@ -14,7 +14,8 @@ import numpy as np
 import pytest
 
 from symmetry_b200 import configs
-from symmetry_b200.lib import Lattice, Server, footprint, job_spec, setup_workload
+from symmetry_b200.lib import (DEV_TIMEOUT, Lattice, Server, footprint, job_spec, selftest_wait_timeout,
+                              setup_workload)
 
 pytestmark = pytest.mark.gpu
 
@@ -175,3 +176,19 @@ def test_drift_and_wall_budget_retire_jobs():
     assert ra.status == 4 and ra.error == 9, ra.as_dict()
     assert rb.status == 4 and rb.error == 5, rb.as_dict()
     assert rc.status == 3 and rc.steps == 60, rc.as_dict()
+
+
+def test_bounded_tile_wait_times_out():
+    """The bounded mbarrier wait of the fused kernels' tile loads gives up on a
+    barrier that nothing arrives on and reports the timeout flag instead of
+    hanging; a completed barrier is seen at once.  The full poll limit of the
+    kernels (2^22 polls) must end within seconds.  A run without faults
+    records no flag."""
+    f1, ms1 = selftest_wait_timeout(256)
+    f2, ms2 = selftest_wait_timeout(4096)
+    assert f1 == DEV_TIMEOUT and f2 == DEV_TIMEOUT, (f1, f2)
+    per_poll_ms = max(ms2 - ms1, 1e-6) / (4096 - 256)
+    assert per_poll_ms * 2 ** 22 < 30_000.0, per_poll_ms
+    L = setup_workload(configs.c1_thread(nx=16, ny=16, nz=32, radius=4.0, storage="fp64"))
+    L.step(20)
+    assert L.device_status() == 0
