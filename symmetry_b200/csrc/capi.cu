@@ -251,6 +251,18 @@ int alloc_state(sym_handle* h) {
 
 }  // namespace
 
+namespace symb200 {
+// calmacros of the current populations into the canonical macro arrays
+// (rho, u, rho_N) without changing the stepping state: from the fused
+// populations when they are current, else from ri/bi (the canonical kernel
+// also writes fi, which CONFIG handles without particles allocate lazily)
+int current_macros(sym_handle* h) {
+  if (h->fast.valid) return fast_macros(h);
+  if (int e = ensure_full(h)) return e;
+  return ref_calmacros(h);
+}
+}  // namespace symb200
+
 extern "C" {
 
 int sym_params_reference(sym_params* p, int nx, int ny, int nz) {
@@ -430,11 +442,7 @@ int sym_get_field(sym_handle* h, int field, void* host) {
 
 int sym_get_macros(sym_handle* h, double* rho, double* ux, double* uy, double* uz, double* rho_n) {
   if (int e = guard(h)) return e;
-  if (h->fast.valid) {
-    if (int e = fast_macros(h)) return e;
-  } else {
-    if (int e = ref_calmacros(h)) return e;
-  }
+  if (int e = current_macros(h)) return e;
   double* src[5] = {h->rho, h->ux, h->uy, h->uz, h->rhoN};
   double* dst[5] = {rho, ux, uy, uz, rho_n};
   for (int k = 0; k < 5; k++)

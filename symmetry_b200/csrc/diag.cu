@@ -85,10 +85,7 @@ __global__ void k_energy_final(const double* part, long long nblk, double* out) 
 
 // the macroscopic fields of the current populations (calmacros) in the
 // canonical arrays, without changing the stepping state
-int macros(sym_handle* h) {
-  if (h->fast.valid) return fast_macros(h);
-  return ref_calmacros(h);
-}
+int macros(sym_handle* h) { return current_macros(h); }
 
 // output4's halving of a particle that starts on a mirror plane (:1765-1779)
 double mirror_factor(const sym_handle* h, const sym_particles& s, int pp) {

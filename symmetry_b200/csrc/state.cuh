@@ -117,6 +117,7 @@ void fast_free(sym_handle* h);
 int fast_import(sym_handle* h);   // canonical -> fast
 int fast_export(sym_handle* h);   // fast -> canonical
 int fast_macros(sym_handle* h);   // calmacros of the fused populations into rho, u, rho_N (fused state kept)
+int current_macros(sym_handle* h);   // calmacros of whichever state is current (capi.cu)
 int fast_step(sym_handle* h, int nsteps);
 int fast_step_timed(sym_handle* h, int nsteps, double ms[4]);
 int fast_neck_planes(sym_handle* h, double* out, cudaStream_t st);   // per-z red area, nz doubles

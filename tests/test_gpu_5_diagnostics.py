@@ -177,3 +177,24 @@ def test_neck_log_reference_geometry(tmp_path):
     assert rows[0].strip() == "VARIABLES=t,t*,h,y0"
     v = np.array(rows[1].split(), dtype=float)
     assert int(v[0]) == 0 and abs(v[2] - h0 / 30.0) < 1e-6 and abs(v[3] - y0 / 172.0) < 1e-6
+
+
+@pytest.mark.parametrize("storage", ["fp64", "fp16"])
+def test_get_macros_fused_and_exported_agree(storage):
+    """sym_get_macros reads the fused populations while they are current and
+    the canonical ones after an export; on a periodic handle without
+    particles the canonical path allocates its calmacros arrays on first use.
+    Both readings of the same state agree (FP64 export is exact; the 16-bit
+    decode is the same function in both)."""
+    w = configs.c1_thread(nx=16, ny=16, nz=32, radius=4.0, storage=storage)
+    L = setup_workload(w)
+    m0 = L.macros()                      # before any step: canonical path
+    assert np.isfinite(m0["rho"]).all()
+    L.step(12)
+    fused = {k: v.copy() for k, v in L.macros().items()}
+    L.mass_momentum()                    # exports: the canonical arrays become current
+    exported = L.macros()
+    for k in ("rho", "ux", "uy", "uz", "rho_N"):
+        a, b = exported[k], fused[k]
+        assert np.abs(a - b).max() <= 1e-13 * max(1.0, np.abs(b).max()), k
+    L.close()
