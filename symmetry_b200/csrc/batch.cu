@@ -78,9 +78,9 @@ __global__ void __launch_bounds__(256) k_finalize_batch(const DomainDesc* __rest
   const DomainDesc& D = descs[e.x];
   const long long L = (long long)e.y * 256 + threadIdx.x;
   if (D.solid)
-    finalize_node<S, true>(D.P, D.pd, (AT*)D.acc, (R*)D.phic, D.walls_all, D.rr_new, D.status, L);
+    finalize_nodes<S, true, 1>(D.P, D.pd, (AT*)D.acc, (R*)D.phic, D.walls_all, D.rr_new, D.status, L);
   else
-    finalize_node<S, false>(D.P, D.pd, (AT*)D.acc, (R*)D.phic, D.walls_all, D.rr_new, D.status, L);
+    finalize_nodes<S, false, 1>(D.P, D.pd, (AT*)D.acc, (R*)D.phic, D.walls_all, D.rr_new, D.status, L);
 }
 
 template <typename S>

@@ -89,12 +89,13 @@ int enqueue_step(sym_handle* h, int cur, int pc, cudaEvent_t* ev) {
   // accumulated, or from the populations
   if (ev) cudaEventRecord(ev[0], h->st);
   if constexpr (kAccumulate<S>) {
+    const unsigned fin_blocks = blocks_for(P.N, 256 * kFinalizeNPT);
     if (solid)
-      k_finalize<S, true><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, accbuf<S>(h), phic, h->walls_all, rr_new(h, pc),
-                                                              h->fast.status);
+      k_finalize<S, true><<<fin_blocks, 256, 0, h->st>>>(P, pd, accbuf<S>(h), phic, h->walls_all, rr_new(h, pc),
+                                                         h->fast.status);
     else
-      k_finalize<S, false><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, accbuf<S>(h), phic, h->walls_all,
-                                                               rr_new(h, pc), h->fast.status);
+      k_finalize<S, false><<<fin_blocks, 256, 0, h->st>>>(P, pd, accbuf<S>(h), phic, h->walls_all, rr_new(h, pc),
+                                                          h->fast.status);
   } else {
     if (solid)
       k_phase<S, true><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, pin_, phic, h->walls_all, rr_old(h, pc),

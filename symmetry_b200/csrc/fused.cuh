@@ -31,19 +31,22 @@ inline Pad make_pad(const DevParams& P) {
 }
 
 // store v at (x,y,z) and at each periodic image inside the 2-deep ghost layers
+// (per axis: the node, +n when it is within 2 of the low face, -n within 2 of
+// the high face; both for n = 3).  The loops unroll completely, so the offsets
+// stay in registers.
 template <typename R>
 __device__ __forceinline__ void phi_store(const DevParams& P, const Pad& pd, R* phi, int x, int y, int z, R v) {
-  int xs[3], ys[3], zs[3], nx = 1, ny = 1, nz = 1;
-  xs[0] = x; ys[0] = y; zs[0] = z;
-  if (x < 2) xs[nx++] = x + P.nx;
-  if (x >= P.nx - 2) xs[nx++] = x - P.nx;
-  if (y < 2) ys[ny++] = y + P.ny;
-  if (y >= P.ny - 2) ys[ny++] = y - P.ny;
-  if (z < 2) zs[nz++] = z + P.nz;
-  if (z >= P.nz - 2) zs[nz++] = z - P.nz;
-  for (int a = 0; a < nx; a++)
-    for (int b = 0; b < ny; b++)
-      for (int c = 0; c < nz; c++) phi[pd.idx(xs[a], ys[b], zs[c])] = v;
+  const long long sx = (long long)pd.nzp * pd.nyp, sy = pd.nzp;
+  const bool on[3][3] = {{true, x < 2, x >= P.nx - 2}, {true, y < 2, y >= P.ny - 2}, {true, z < 2, z >= P.nz - 2}};
+  const long long ox[3] = {0, P.nx * sx, -P.nx * sx}, oy[3] = {0, P.ny * sy, -P.ny * sy}, oz[3] = {0, P.nz, -P.nz};
+  R* const p0 = phi + pd.idx(x, y, z);
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++)
+#pragma unroll
+      for (int c = 0; c < 3; c++)
+        if (on[0][a] && on[1][b] && on[2][c]) p0[ox[a] + oy[b] + oz[c]] = v;
 }
 
 // ---- population storage codecs --------------------------------------------------
@@ -209,7 +212,7 @@ __device__ __forceinline__ void unroll19(F&& f) {
 // ---- calmacros (Source1.f90:770-831) on the fused state ---------------------------
 // Storages that do not accumulate: phi = (rhoR - rhoB) / rho from the node's
 // own post-stream populations; 0 on solid nodes.  16-bit storage decodes with
-// rr_old and records 1/rho in rr_new (as finalize_node below).
+// rr_old and records 1/rho in rr_new (as finalize_nodes below).
 template <typename S, bool SOLID>
 __device__ __forceinline__ void phase_node(const DevParams& P, const Pad& pd, const S* __restrict__ pops,
                                            typename Codec<S>::R* __restrict__ phi,
@@ -253,38 +256,63 @@ __global__ void __launch_bounds__(256) k_phase(DevParams P, Pad pd, const S* __r
 // of this step.  16-bit storage also records 1/rho (1/rho0 on solid nodes) in
 // rr_new: the reference density this step's encoders use and the next step
 // decodes with (rr_new here, rr_old there: both hold 1/rho_ref).
-template <typename S, bool SOLID>
-__device__ __forceinline__ void finalize_node(const DevParams& P, const Pad& pd,
-                                              typename Acc<typename Codec<S>::R>::T* acc,
-                                              typename Codec<S>::R* __restrict__ phi,
-                                              const int32_t* __restrict__ walls_all, float* __restrict__ rr_new,
-                                              const int* __restrict__ status, long long L) {
+// Nodes L0, L0 + 256, ..., L0 + 256 (NPT-1) per thread: every load of all of
+// them is issued before the first store, so a thread keeps 2 NPT accumulator
+// reads in flight (nothing waits on a store).
+template <typename S, bool SOLID, int NPT>
+__device__ __forceinline__ void finalize_nodes(const DevParams& P, const Pad& pd,
+                                               typename Acc<typename Codec<S>::R>::T* __restrict__ acc,
+                                               typename Codec<S>::R* __restrict__ phi,
+                                               const int32_t* __restrict__ walls_all, float* __restrict__ rr_new,
+                                               const int* __restrict__ status, long long L0) {
   using R = typename Codec<S>::R;
   using A = Acc<R>;
-  if (L >= P.N) return;
-  // 32-bit index arithmetic (the fused path keeps 38*N < 2^32)
-  const unsigned Lu = (unsigned)L, q = Lu / (unsigned)P.nz;
-  const int z = (int)(Lu - q * (unsigned)P.nz), x = (int)(q / (unsigned)P.ny), y = (int)(q - (unsigned)x * P.ny);
-  const R sr = A::val(acc[L]), sb = A::val(acc[L + P.N]);
-  acc[L] = 0;
-  acc[L + P.N] = 0;
-  R v = R(0);
-  R rho = R(P.rho0);
-  if (!(SOLID && walls_all[L] >= 1)) {
-    rho = sr + sb;
-    v = qdiv<R>(sr - sb, rho);
+  const int bad = *status;
+  typename A::T ar[NPT], ab[NPT];
+  bool solid[NPT];
+#pragma unroll
+  for (int k = 0; k < NPT; k++) {
+    const long long L = L0 + 256LL * k;
+    ar[k] = ab[k] = 0;
+    solid[k] = false;
+    if (L < P.N) {
+      ar[k] = acc[L];
+      ab[k] = acc[L + P.N];
+      solid[k] = SOLID && walls_all[L] >= 1;
+    }
   }
-  if (*status) v = R(NAN);
-  phi_store<R>(P, pd, phi, x, y, z, v);
-  if (Codec<S>::kRef) phi_store<float>(P, pd, rr_new, x, y, z, 1.0f / float(rho));
+#pragma unroll
+  for (int k = 0; k < NPT; k++) {
+    const long long L = L0 + 256LL * k;
+    if (L >= P.N) break;
+    acc[L] = 0;
+    acc[L + P.N] = 0;
+    // 32-bit index arithmetic (the fused path keeps 38*N < 2^32)
+    const unsigned Lu = (unsigned)L, q = Lu / (unsigned)P.nz;
+    const int z = (int)(Lu - q * (unsigned)P.nz), x = (int)(q / (unsigned)P.ny), y = (int)(q - (unsigned)x * P.ny);
+    const R sr = A::val(ar[k]), sb = A::val(ab[k]);
+    R v = R(0);
+    R rho = R(P.rho0);
+    if (!solid[k]) {
+      rho = sr + sb;
+      v = qdiv<R>(sr - sb, rho);
+    }
+    if (bad) v = R(NAN);
+    phi_store<R>(P, pd, phi, x, y, z, v);
+    if (Codec<S>::kRef) phi_store<float>(P, pd, rr_new, x, y, z, 1.0f / float(rho));
+  }
 }
+
+// nodes finalised per thread by the single-domain kernel
+constexpr int kFinalizeNPT = 4;
 
 template <typename S, bool SOLID>
 __global__ void __launch_bounds__(256) k_finalize(DevParams P, Pad pd, typename Acc<typename Codec<S>::R>::T* acc,
                                                   typename Codec<S>::R* __restrict__ phi,
                                                   const int32_t* __restrict__ walls_all, float* __restrict__ rr_new,
                                                   const int* __restrict__ status) {
-  finalize_node<S, SOLID>(P, pd, acc, phi, walls_all, rr_new, status, blockIdx.x * 256LL + threadIdx.x);
+  finalize_nodes<S, SOLID, kFinalizeNPT>(P, pd, acc, phi, walls_all, rr_new, status,
+                                         blockIdx.x * (256LL * kFinalizeNPT) + threadIdx.x);
 }
 
 // ---- wetting rotation of a node normal (derivatives :535-587) ---------------------
@@ -531,8 +559,10 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
     // accumulating kernels run every lane of a warp with an active node (the
     // shuffles need the whole warp); the others skip inactive nodes
     if (ACC ? __any_sync(0xffffffffu, act) : act) {
-    if (x + 1 < xb) {
-      // bring the next plane's populations toward L2 while this plane computes
+    if (sizeof(R) == 8 && x + 1 < xb) {
+      // FP64: bring the next plane's populations toward L2 while this plane
+      // computes (the FP32-math kernels, bound by instruction issue, measured
+      // faster without the 19 prefetch instructions)
 #pragma unroll
       for (int i = 0; i < 19; i++) asm volatile("prefetch.global.L2 [%0];" ::"l"(pin_ + 2 * (i * N + L + sx)));
     }
@@ -722,10 +752,11 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
 }
 
 // Resident CTAs per SM the collide kernels are compiled for: the FP32-math
-// codecs fit 80 registers without spilling (3 CTAs of 256 threads), FP64
+// codecs fit 64 registers (4 CTAs of 256 threads; measured faster than 3 CTAs
+// at 80 registers, the issue-bound kernel gains from the extra warps), FP64
 // needs the 128 of 2 CTAs.
 template <typename S>
-constexpr int collide_ctas() { return sizeof(typename Codec<S>::R) == 4 ? 3 : 2; }
+constexpr int collide_ctas() { return sizeof(typename Codec<S>::R) == 4 ? 4 : 2; }
 
 template <typename S, bool SOLID>
 __global__ void __launch_bounds__(TPB, collide_ctas<S>()) k_collide(DevParams P, Pad pd, const S* __restrict__ pin_,
