@@ -241,9 +241,10 @@ int sym_step_timed(sym_handle* h, int nsteps, int use_graph, double ms[4]);
  * No counterpart in the reference (it runs one domain).  A batch references
  * existing handles (same device, CONFIG mode, same storage) and steps them in
  * lockstep: one CUDA graph per step containing one phase-field launch for all
- * domains, the per-domain particle/wall work, and one persistent collide
- * launch whose CTAs pull 32x8xX tiles of any domain from a work-tile table
- * (largest first).  Results per domain are identical to sym_step on that
+ * domains, the particle and wall work of all domains (one launch per
+ * subroutine over a (domain, particle, block) table), and one persistent
+ * collide launch whose CTAs pull 32x8xX tiles of any domain from a work-tile
+ * table (largest first).  Results per domain are identical to sym_step on that
  * domain alone with the same tile x extent.  Member handles stay usable on
  * their own; the batch rebuilds its graphs when a member was stepped or read
  * back outside it. */
@@ -256,8 +257,12 @@ int sym_batch_step(sym_batch* b, int nsteps);
 int sym_batch_step_timed(sym_batch* b, int nsteps, double* ms);
 int sym_batch_set_xchunk(sym_batch* b, int domain, int xchunk);
 int sym_batch_get_xchunk(sym_batch* b, int domain, int* xchunk);
+/* Resident collide CTAs per SM of the persistent launch (1 .. the most that
+ * fit; default the most): grid = per_sm x SM count. */
+int sym_batch_set_ctas_per_sm(sym_batch* b, int per_sm);
 /* Picks the tile x extent per size class (nx <= 32, <= 48, larger) from
- * {8,16,32,64} by timing; the trial steps advance every domain (*steps_taken). */
+ * {8,16,32,64}, then the resident CTAs per SM, by timing; the trial steps
+ * advance every domain (*steps_taken). */
 int sym_batch_autotune(sym_batch* b, int trial_steps, int* steps_taken);
 int sym_batch_info(sym_batch* b, int64_t* nodes, int* ntiles, int* grid);
 /* nsteps eager batch steps (not the graph) with CUDA events on the batch

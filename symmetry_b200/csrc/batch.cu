@@ -118,16 +118,17 @@ __global__ void __launch_bounds__(kTPB, collide_ctas<S>()) k_collide_batch(const
   }
 }
 
+// the collide kernel's dynamic shared memory, and how many of its CTAs fit
+// on one SM (*per_sm) of the device's *sms
 template <typename S>
-int set_batch_smem(cudaStream_t, int* grid_blocks, int device) {
-  using R = typename Codec<S>::R;
+int set_batch_smem(int device, int* per_sm, int* sms) {
   const int shm = (int)smem_bytes<S>();
   if (cudaFuncSetAttribute(k_collide_batch<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, shm) != cudaSuccess)
     return SYM_ERR_CUDA;
-  int per_sm = 0, sms = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_collide_batch<S>, kTPB, shm);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  *grid_blocks = std::max(1, per_sm) * std::max(1, sms);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_collide_batch<S>, kTPB, shm);
+  cudaDeviceGetAttribute(sms, cudaDevAttrMultiProcessorCount, device);
+  *per_sm = std::max(1, *per_sm);
+  *sms = std::max(1, *sms);
   return SYM_OK;
 }
 
@@ -148,7 +149,8 @@ struct sym_batch {
   int ntiles = 0;
   long long nblocks = 0;
   int* d_counter = nullptr;
-  int grid = 0;
+  int grid = 0;                   // persistent collide CTAs: per_sm x sms
+  int sms = 0, max_per_sm = 0, per_sm = 0;
   SparsePlan* sparse = nullptr;   // particle and wall work of every domain, batched
   cudaGraph_t graph[2] = {nullptr, nullptr};
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
@@ -384,9 +386,11 @@ int sym_batch_create(sym_handle* const* handles, int n, sym_batch** out) {
   int e = bcuda(b, cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking), "stream");
   if (!e) e = bcuda(b, cudaMalloc(&b->d_counter, 2 * sizeof(int)), "counter");
   if (!e) {
-    e = b->storage == SYM_STORE_FP64 ? set_batch_smem<double>(b->st, &b->grid, b->device)
-      : b->storage == SYM_STORE_FP32 ? set_batch_smem<float>(b->st, &b->grid, b->device)
-                                     : set_batch_smem<__half>(b->st, &b->grid, b->device);
+    e = b->storage == SYM_STORE_FP64 ? set_batch_smem<double>(b->device, &b->max_per_sm, &b->sms)
+      : b->storage == SYM_STORE_FP32 ? set_batch_smem<float>(b->device, &b->max_per_sm, &b->sms)
+                                     : set_batch_smem<__half>(b->device, &b->max_per_sm, &b->sms);
+    b->per_sm = b->max_per_sm;
+    b->grid = b->per_sm * b->sms;
   }
   if (e) {
     fprintf(stderr, "sym_batch_create: %s\n", b->err.c_str());
@@ -417,6 +421,16 @@ int sym_batch_set_xchunk(sym_batch* b, int domain, int xchunk) {
   if (!b || domain < 0 || domain >= (int)b->doms.size() || xchunk < 1) return SYM_ERR_PARAM;
   if (b->xchunk[domain] != xchunk) {
     b->xchunk[domain] = xchunk;
+    free_graphs(b);
+  }
+  return SYM_OK;
+}
+
+int sym_batch_set_ctas_per_sm(sym_batch* b, int per_sm) {
+  if (!b || per_sm < 1 || per_sm > b->max_per_sm) return SYM_ERR_PARAM;
+  if (b->per_sm != per_sm) {
+    b->per_sm = per_sm;
+    b->grid = per_sm * b->sms;
     free_graphs(b);
   }
   return SYM_OK;
@@ -458,9 +472,10 @@ int sym_batch_step_timed(sym_batch* b, int nsteps, double* ms) {
 }
 
 // Choose the tile x extent per size class (domains grouped by nx: <=32, <=48,
-// larger) from {8, 16, 32, 64} by timing trial_steps graph steps per
-// candidate.  The trial steps advance every domain; *steps_taken reports how
-// many.
+// larger) from {8, 16, 32, 64}, then the persistent collide grid (resident
+// CTAs per SM, from the most that fit down to 1), each by timing trial_steps
+// graph steps per candidate.  The trial steps advance every domain;
+// *steps_taken reports how many.
 int sym_batch_autotune(sym_batch* b, int trial_steps, int* steps_taken) {
   if (!b || trial_steps <= 0) return SYM_ERR_PARAM;
   const int cands[4] = {8, 16, 32, 64};
@@ -485,6 +500,18 @@ int sym_batch_autotune(sym_batch* b, int trial_steps, int* steps_taken) {
     for (size_t i = 0; i < b->doms.size(); i++)
       if (cls(b->doms[i]->dp.nx) == c) sym_batch_set_xchunk(b, (int)i, bestx);
   }
+  double best = 1e300;
+  int bestc = b->max_per_sm;
+  for (int c = b->max_per_sm; c >= 1; c--) {
+    sym_batch_set_ctas_per_sm(b, c);
+    double ms = 0;
+    if (int e = sym_batch_step(b, 1)) return e;
+    taken += 1;
+    if (int e = sym_batch_step_timed(b, trial_steps, &ms)) return e;
+    taken += trial_steps;
+    if (ms < best) { best = ms; bestc = c; }
+  }
+  sym_batch_set_ctas_per_sm(b, bestc);
   if (steps_taken) *steps_taken = taken;
   return SYM_OK;
 }

@@ -31,22 +31,25 @@ inline Pad make_pad(const DevParams& P) {
 }
 
 // store v at (x,y,z) and at each periodic image inside the 2-deep ghost layers
-// (per axis: the node, +n when it is within 2 of the low face, -n within 2 of
-// the high face; both for n = 3).  The loops unroll completely, so the offsets
-// stay in registers.
+// (per axis: +n when within 2 of the low face, -n within 2 of the high face;
+// both for n = 3).  Nodes 2 or more from every face store once.
 template <typename R>
 __device__ __forceinline__ void phi_store(const DevParams& P, const Pad& pd, R* phi, int x, int y, int z, R v) {
-  const long long sx = (long long)pd.nzp * pd.nyp, sy = pd.nzp;
-  const bool on[3][3] = {{true, x < 2, x >= P.nx - 2}, {true, y < 2, y >= P.ny - 2}, {true, z < 2, z >= P.nz - 2}};
-  const long long ox[3] = {0, P.nx * sx, -P.nx * sx}, oy[3] = {0, P.ny * sy, -P.ny * sy}, oz[3] = {0, P.nz, -P.nz};
-  R* const p0 = phi + pd.idx(x, y, z);
-#pragma unroll
-  for (int a = 0; a < 3; a++)
-#pragma unroll
-    for (int b = 0; b < 3; b++)
-#pragma unroll
-      for (int c = 0; c < 3; c++)
-        if (on[0][a] && on[1][b] && on[2][c]) p0[ox[a] + oy[b] + oz[c]] = v;
+  if (x >= 2 && x < P.nx - 2 && y >= 2 && y < P.ny - 2 && z >= 2 && z < P.nz - 2) {
+    phi[pd.idx(x, y, z)] = v;
+    return;
+  }
+  int xs[3], ys[3], zs[3], nx = 1, ny = 1, nz = 1;
+  xs[0] = x; ys[0] = y; zs[0] = z;
+  if (x < 2) xs[nx++] = x + P.nx;
+  if (x >= P.nx - 2) xs[nx++] = x - P.nx;
+  if (y < 2) ys[ny++] = y + P.ny;
+  if (y >= P.ny - 2) ys[ny++] = y - P.ny;
+  if (z < 2) zs[nz++] = z + P.nz;
+  if (z >= P.nz - 2) zs[nz++] = z - P.nz;
+  for (int a = 0; a < nx; a++)
+    for (int b = 0; b < ny; b++)
+      for (int c = 0; c < nz; c++) phi[pd.idx(xs[a], ys[b], zs[c])] = v;
 }
 
 // ---- population storage codecs --------------------------------------------------
@@ -355,9 +358,9 @@ struct Smem {
   alignas(128) R phi[5][kPhiSlot];
   alignas(128) float irr[Codec<S>::kRef ? kIrrRing : 1][kIrrSlot];   // 1/rho_ref of this step (16-bit storage)
   NormalV<R> n[4][BY + 2][BZ + 2];   // [plane][y][z]: n and |grad phi|
-  // [plane parity][cx+1][to row y+1, y-1][colour]: density sums crossing rows
-  // (accumulating storages; written at one plane, read after the next plane's barrier)
-  R xch[kAccumulate<S> ? 2 : 1][kAccumulate<S> ? 3 : 1][2][2][kAccumulate<S> ? BY : 1][kAccumulate<S> ? BZ : 1];
+  // [cx+1][to row y+1, y-1][colour]: density sums crossing rows (accumulating
+  // storages only; a single element otherwise)
+  R xch[kAccumulate<S> ? 3 : 1][2][2][kAccumulate<S> ? BY : 1][kAccumulate<S> ? BZ : 1];
   uint64_t bar[kIrrRing];   // one mbarrier per plane load, used round robin
 };
 // dynamic shared memory of the collide kernels: the Smem block on a 128-byte
@@ -434,7 +437,11 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
   auto PHI = [&](int xp, int py, int pz) -> R { return sm.phi[((xp % 5) + 5) % 5][py * (BZ + 4) + pz]; };
   // unit normal (rotated at wetting nodes) and |grad phi| of plane xp, halo 1
   auto compute_n = [&](int xp) {
-    const int s = ((xp % 4) + 4) % 4;
+    const int s = xp & 3;   // xp >= -1: the slot in the 4-plane normal ring
+    // phi planes xp-1, xp, xp+1 in the 5-plane ring (xp >= -1)
+    const R* const pm = sm.phi[(unsigned)(xp + 4) % 5u];
+    const R* const p0 = sm.phi[(unsigned)(xp + 5) % 5u];
+    const R* const pp1 = sm.phi[(unsigned)(xp + 6) % 5u];
     for (int t = threadIdx.x; t < (BY + 2) * (BZ + 2); t += TPB) {
       const int py = t / (BZ + 2), pz = t % (BZ + 2);
       const int y = y0 - 1 + py, z = z0 - 1 + pz;
@@ -452,19 +459,28 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
         R g0 = R(0), g1 = R(0), g2 = R(0);
         static_for<9>([&](auto kc) {
           constexpr int i = PREP(decltype(kc)::value);
-          const R d = PHI(xp + CX(i), py + 1 + CY(i), pz + 1 + CZ(i)) - PHI(xp - CX(i), py + 1 - CY(i), pz + 1 - CZ(i));
+          constexpr int o = CY(i) * (BZ + 4) + CZ(i);
+          const int b = (py + 1) * (BZ + 4) + pz + 1;
+          const R* const pa = CX(i) > 0 ? pp1 : (CX(i) < 0 ? pm : p0);
+          const R* const pb = CX(i) > 0 ? pm : (CX(i) < 0 ? pp1 : p0);
+          const R d = pa[b + o] - pb[b - o];
           if (CX(i)) g0 = g0 + R(W(i) * CX(i)) * d;
           if (CY(i)) g1 = g1 + R(W(i) * CY(i)) * d;
           if (CZ(i)) g2 = g2 + R(W(i) * CZ(i)) * d;
         });
         g0 = R(3) * g0; g1 = R(3) * g1; g2 = R(3) * g2;
-        fn = sqrt(g0 * g0 + g1 * g1 + g2 * g2);
-        if (fn > evap) {
-          const R rf = qdiv<R>(R(1), fn);
+        const R g2s = g0 * g0 + g1 * g1 + g2 * g2;
+        R rf = R(0);
+        if constexpr (sizeof(R) == 4) {
+          // FP32 arithmetic: |grad phi| and its reciprocal from one rsqrt
+          if (g2s > evap * evap) { rf = rsqrtf(g2s); fn = g2s * rf; }
+        } else {
+          fn = sqrt(g2s);
+          if (fn > evap) rf = R(1) / fn; else fn = R(0);
+        }
+        if (fn > R(0)) {
           n0 = g0 * rf; n1 = g1 * rf; n2 = g2 * rf;
           if (SOLIDX && pp >= 1) wet_rotate<R>(P, Sp, pp, wrapi(xp, P.nx), wrapi(y, P.ny), wrapi(z, P.nz), n0, n1, n2);
-        } else {
-          fn = R(0);
         }
       }
       sm.n[s][py][pz] = NormalV<R>{n0, n1, n2, fn};
@@ -496,37 +512,7 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
   using AT = typename Acc<R>::T;
   AT* const accR = acc;
   AT* const accB = acc + N;
-  R aPr = R(0), aPb = R(0), aCr = R(0), aCb = R(0), aNr = R(0), aNb = R(0);   // planes k-1, k, k+1
-  R gk[3][2];   // this column's own sums of plane k (cy = 0, bounce-backs), kept for the combine
-  // Combine the in-tile sums computed at plane k -- own sums gk plus the
-  // cy = +-1 sums the neighbouring rows left in xch[k & 1] -- into the planes
-  // k-1, k, k+1 of this column; plane k-1 then has all its in-tile
-  // contributions and is added to the accumulators.  Runs after the barrier
-  // that follows plane k's writes (the next plane's, or the final one).
-  auto combine = [&](int k) {
-    const int q = k & 1;
-    R in[3][2];
-#pragma unroll
-    for (int a = 0; a < 3; a++)
-#pragma unroll
-      for (int c = 0; c < 2; c++) {
-        R v = gk[a][c];
-        if (ty > 0) v = v + sm.xch[q][a][0][c][ty - 1][tz];
-        if (ty < BY - 1) v = v + sm.xch[q][a][1][c][ty + 1][tz];
-        in[a][c] = v;
-      }
-    aPr = aPr + in[0][0]; aPb = aPb + in[0][1];
-    aCr = aCr + in[1][0]; aCb = aCb + in[1][1];
-    aNr = aNr + in[2][0]; aNb = aNb + in[2][1];
-    if (k > xa && inr && (aPr != R(0) || aPb != R(0))) {
-      const unsigned Lp = (unsigned)(z + sy * y + sx * (k - 1));
-      acc_add<R>(accR + Lp, aPr, status);
-      acc_add<R>(accB + Lp, aPb, status);
-    }
-    aPr = aCr; aPb = aCb;
-    aCr = aNr; aCb = aNb;
-    aNr = R(0); aNb = R(0);
-  };
+  R aPr = R(0), aPb = R(0), aCr = R(0), aCb = R(0), aNr = R(0), aNb = R(0);   // planes x-1, x, x+1
   for (int x = xa; x < xb; x++) {
     // phi of plane x+3 on its way; normals of plane x+1 from phi planes x..x+2.
     // The slots the load overwrites (phi of plane x-2, 1/rho_ref of plane x-3)
@@ -535,9 +521,6 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
     wait_phi(x + 2);
     compute_n(x + 1);
     __syncthreads();
-    if constexpr (ACC) {
-      if (x > xa) combine(x - 1);
-    }
     const unsigned L = (unsigned)(zc + sy * yc + sx * x);
     int pp = 0;
     bool act = inr;
@@ -588,8 +571,7 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
     }
     const R irho = qdiv<R>(R(1), rho);
     ux = ux * irho; uy = uy * irho; uz = uz * irho;
-    const int s1 = x % 4;
-    const NormalV<R> nown = sm.n[s1][ty + 1][tz + 1];
+    const NormalV<R> nown = sm.n[x & 3][ty + 1][tz + 1];
     const R nx = nown.x, ny = nown.y, nz = nown.z, fn = nown.g;
     const bool flag = fn > evap;
     const R rhoN = PHI(x, ty + 2, tz + 2);
@@ -601,8 +583,8 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
       R d00 = 0, d01 = 0, d02 = 0, d10 = 0, d11 = 0, d12 = 0, d20 = 0, d21 = 0, d22 = 0;
       static_for<9>([&](auto kc) {
         constexpr int i = PREP(decltype(kc)::value);
-        const NormalV<R> p = sm.n[(x + CX(i) + 4) % 4][ty + 1 + CY(i)][tz + 1 + CZ(i)];
-        const NormalV<R> m = sm.n[(x - CX(i) + 4) % 4][ty + 1 - CY(i)][tz + 1 - CZ(i)];
+        const NormalV<R> p = sm.n[(x + CX(i)) & 3][ty + 1 + CY(i)][tz + 1 + CZ(i)];
+        const NormalV<R> m = sm.n[(x - CX(i)) & 3][ty + 1 - CY(i)][tz + 1 - CZ(i)];
         const R a = p.x - m.x, b = p.y - m.y, c = p.z - m.z;
         if (CX(i)) { constexpr double k = W(i) * CX(i); d00 = d00 + R(k) * a; d10 = d10 + R(k) * b; d20 = d20 + R(k) * c; }
         if (CY(i)) { constexpr double k = W(i) * CY(i); d01 = d01 + R(k) * a; d11 = d11 + R(k) * b; d21 = d21 + R(k) * c; }
@@ -679,7 +661,7 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
             const R star = flat ? R(0) : uw0 * R(CX(j)) + uw1 * R(CY(j)) + uw2 * R(CZ(j));
             const R rr = r + R(6.0 * W(j)) * sr * star;
             const R bb = (f[i] - r) + R(6.0 * W(j)) * sb * star;
-            const R irr = REF ? R(sm.irr[x % kIrrRing][(ty + 2) * (BZ + 4) + tz + 2]) : irho0;
+            const R irr = REF ? R(sm.irr[(unsigned)x % kIrrRing][(ty + 2) * (BZ + 4) + tz + 2]) : irho0;
             Codec<S>::template store<j>(pout_, N, L, irr, rr, rr + bb);
             sfr = sfr + rr;
             sfb = sfb + bb;
@@ -687,7 +669,8 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
           }
         }
         const R irr =
-            REF ? R(sm.irr[(x + CX(i) + kIrrRing) % kIrrRing][(ty + 2 + CY(i)) * (BZ + 4) + tz + 2 + CZ(i)]) : irho0;
+            REF ? R(sm.irr[(unsigned)(x + CX(i) + kIrrRing) % kIrrRing][(ty + 2 + CY(i)) * (BZ + 4) + tz + 2 + CZ(i)])
+                : irho0;
         Codec<S>::template store<i>(pout_, N, T, irr, r, f[i]);
         if constexpr (!ACC) return;
         const R bv = f[i] - r;
@@ -722,26 +705,37 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
     });
     }
     if constexpr (ACC) {
-      // along y through shared memory: row ty+1 takes the cy = +1 sums of row
-      // ty and row ty-1 the cy = -1 sums, for each destination plane (read in
-      // the combine after the next barrier)
-      const int q = x & 1;
+      // along y through shared memory: row ty+1 receives the cy = +1 sums of row
+      // ty and row ty-1 the cy = -1 sums, for each destination plane
 #pragma unroll
       for (int a = 0; a < 3; a++)
 #pragma unroll
         for (int c = 0; c < 2; c++) {
-          sm.xch[q][a][0][c][ty][tz] = g[a][2][c];
-          sm.xch[q][a][1][c][ty][tz] = g[a][0][c];
-          gk[a][c] = g[a][1][c];
+          sm.xch[a][0][c][ty][tz] = g[a][2][c];
+          sm.xch[a][1][c][ty][tz] = g[a][0][c];
         }
-      gk[1][0] = gk[1][0] + sfr;
-      gk[1][1] = gk[1][1] + sfb;
-    }
-  }
-  if constexpr (ACC) {
-    if (xb > xa) {
       __syncthreads();
-      combine(xb - 1);
+      R in[3][2];
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int c = 0; c < 2; c++) {
+          R v = g[a][1][c];
+          if (ty > 0) v = v + sm.xch[a][0][c][ty - 1][tz];
+          if (ty < BY - 1) v = v + sm.xch[a][1][c][ty + 1][tz];
+          in[a][c] = v;
+        }
+      aPr = aPr + in[0][0]; aPb = aPb + in[0][1];
+      aCr = aCr + in[1][0] + sfr; aCb = aCb + in[1][1] + sfb;
+      aNr = aNr + in[2][0]; aNb = aNb + in[2][1];
+      // plane x-1 of this column has all its in-tile contributions
+      if (x > xa && inr && (aPr != R(0) || aPb != R(0))) {
+        acc_add<R>(accR + (L - sx), aPr, status);
+        acc_add<R>(accB + (L - sx), aPb, status);
+      }
+      aPr = aCr; aPb = aCb;
+      aCr = aNr; aCb = aNb;
+      aNr = R(0); aNb = R(0);
     }
   }
   if (ACC && xb > xa && inr && (aPr != R(0) || aPb != R(0))) {

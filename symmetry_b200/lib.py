@@ -96,6 +96,7 @@ def lib() -> ctypes.CDLL:
         L.sym_batch_set_xchunk.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
         L.sym_batch_get_xchunk.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
         L.sym_batch_autotune.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+        L.sym_batch_set_ctas_per_sm.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.sym_batch_info.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int),
                                      ctypes.POINTER(ctypes.c_int)]
         L.sym_batch_step_kernels.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
@@ -350,6 +351,9 @@ class Batch:
 
     def set_xchunk(self, i: int, x: int):
         self._ck(lib().sym_batch_set_xchunk(self.b, i, x), "set_xchunk")
+
+    def set_ctas_per_sm(self, c: int):
+        self._ck(lib().sym_batch_set_ctas_per_sm(self.b, c), "set_ctas_per_sm")
 
     def xchunk(self, i: int) -> int:
         v = ctypes.c_int()

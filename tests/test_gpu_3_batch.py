@@ -73,3 +73,21 @@ def test_batch_autotune_and_info():
     # stepping after tuning still matches a domain stepped alone with the same tiles
     B.step(3)
     B.close()
+
+
+def test_batch_grid_size_does_not_change_results():
+    """The persistent collide grid (resident CTAs per SM, an autotuning knob)
+    changes which CTA takes which tile, never a tile's result."""
+    ws = mix("fp64")
+    runs = []
+    for per_sm in (None, 1):
+        members = [setup_workload(w) for w in ws]
+        B = Batch(members)
+        if per_sm:
+            B.set_ctas_per_sm(per_sm)
+            assert B.info()["grid"] % per_sm == 0
+        B.step(12)
+        runs.append([state(m) for m in members])
+        B.close()
+    for w, a, b in zip(ws, runs[0], runs[1]):
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]), w.name
