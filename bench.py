@@ -63,8 +63,26 @@ def b_collide(storage):
 
 
 def b_phase(storage):
-    """Algorithmic bytes per node of the phase kernel: 38 populations read, phi written."""
+    """Bytes per node the phase kernel must move: FP64 reads the two colour
+    densities the collide kernel accumulated, clears them and writes phi;
+    the other storages read the 38 populations and write phi."""
+    if storage == "fp64":
+        return 4 * 8 + PHI_BYTES[storage]
     return 38 * STORE_BYTES[storage] + PHI_BYTES[storage]
+
+
+# DRAM bytes per node of one collide launch, dram__bytes_read.sum +
+# dram__bytes_write.sum from one ncu capture divided by the nodes of the
+# launch: profiles/k_collide_batch_fp16_mix24.md (16-bit, batched kernel) and
+# profiles/k_collide_fp64_thread_128x128x256.md (FP64, single-domain kernel;
+# the batched kernel runs the same tile code).  The traffic per node does not
+# depend on the number of nodes, so it scales to a full launch.
+COLLIDE_TRAFFIC_B_PER_NODE = {"fp16": 219.3, "fp64": 709.1}
+
+
+def collide_traffic(storage, nodes):
+    b = COLLIDE_TRAFFIC_B_PER_NODE.get(storage)
+    return None if b is None else b * nodes
 
 
 def b_step(storage):
@@ -352,6 +370,7 @@ def c3_leg(steps, peak, local):
             "step_gbs": b_step("fp64") * v * 1e6 / 1e9, "step_frac": b_step("fp64") * v * 1e6 / 1e9 / peak,
             "collide_ms": col, "collide_gbs": b_collide("fp64") * n / (col / 1e3) / 1e9,
             "collide_frac": b_collide("fp64") * n / (col / 1e3) / 1e9 / peak,
+            "collide_traffic": collide_traffic("fp64", n),
             "phase_ms": ph, "phase_gbs": b_phase("fp64") * n / (ph / 1e3) / 1e9,
             "phase_frac": b_phase("fp64") * n / (ph / 1e3) / 1e9 / peak}
 
@@ -432,6 +451,9 @@ def main():
     ap.add_argument("--serve-cap", type=int, default=6000)
     ap.add_argument("--serve-wall", type=float, default=120.0)
     ap.add_argument("--serve-budget-gb", type=float, default=160.0)
+    ap.add_argument("--serve-slots", type=int, default=16,
+                    help="resident jobs of the batched server (16 and 48 served the same MLUPS; 16 the shorter "
+                         "time to result; 256 left most jobs unfinished at the wall-clock limit)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -523,7 +545,9 @@ def mix_main(args, torch, dist, rank, world, local, legs, peak, peak_kind):
             line["roofline"] = {
                 "bound": "hbm", "kernel": "k_collide_batch (fused derivatives+collide+recolour+stream, "
                                           "persistent over the work-tile table)",
-                "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak, "traffic": None,
+                "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                "traffic": collide_traffic(storage, nodes),
+                "traffic_source": "ncu dram bytes per node of one captured launch x nodes of this launch",
                 "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
                 "algorithmic_bytes_per_node": b_collide(storage), "nodes_per_launch": nodes,
                 "ms_per_launch": col}
@@ -556,8 +580,8 @@ def mix_main(args, torch, dist, rank, world, local, legs, peak, peak_kind):
                         f"budget {args.serve_budget_gb:.0f} GB, check every 10 steps, wall-clock limit "
                         f"{args.serve_wall:.0f} s per arm: the offered load exceeds capacity, jobs unfinished "
                         "at the limit are the backlog",
-            "batched_fp16": leg("serve16", run_serving, "fp16", 256, 20.0, args.serve_seconds, args.serve_cap,
-                                int(args.serve_budget_gb * 1e9), args.serve_wall, xchunk, local),
+            "batched_fp16": leg("serve16", run_serving, "fp16", args.serve_slots, 20.0, args.serve_seconds,
+                                args.serve_cap, int(args.serve_budget_gb * 1e9), args.serve_wall, xchunk, local),
             "plain_fp64_one_at_a_time": leg("serve64", run_serving, "fp64", 1, 20.0, args.serve_seconds,
                                             args.serve_cap, int(args.serve_budget_gb * 1e9), args.serve_wall,
                                             None, local),
@@ -595,7 +619,7 @@ def single_main(args, torch, dist, rank, world, local, legs, peak, peak_kind):
                    "l2": f"{2 * 38 * STORE_BYTES[storage] * nodes / 1e9:.2f} GB of populations "
                          "(larger than L2 only for the 256x256x512 thread)"},
         "roofline": {"bound": "hbm", "kernel": "k_collide", "achieved": ach, "peak": peak, "unit": "GB/s",
-                     "frac": ach / peak, "traffic": None, "peak_kind": peak_kind,
+                     "frac": ach / peak, "traffic": collide_traffic(storage, nodes), "peak_kind": peak_kind,
                      "algorithmic_bytes_per_node": b_collide(storage), "ms_per_launch": col},
         "per_kernel_ms_per_step": {"k_phase": ph, "sparse": k[2] / ks, "k_collide": col,
                                    "step_frac_graph": b_step(storage) * value * 1e6 / world / 1e9 / peak},

@@ -39,12 +39,12 @@ struct DomainDesc {
   const int32_t* pout;
   const sym_particles* Sp;
   double* ffi;
-  const float* rr_old;  // 16-bit storage: reference densities (see fused.cuh)
-  float* rr_new;
+  const Ref* rr_old;  // 16-bit storage: reference pairs (see fused.cuh)
+  Ref* rr_new;
   void* acc;            // accumulated colour densities of the next step (see fused.cuh)
   int* status;
   const CUtensorMap* tm_phi;    // TMA descriptors (device copies) of this step's phase field
-  const CUtensorMap* tm_rinv;   // and 1/rho_ref arrays
+  const CUtensorMap* tm_ref;   // and reference-pair arrays
   int solid;
   int pad_;
 };
@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(kTPB, collide_ctas<S>()) k_collide_batch(const
     // domain): the instruction working set of the persistent kernel stays
     // that of one variant
     collide_tile<S, true>(D.P, D.pd, (const S*)D.pin, (S*)D.pnext, (const R*)D.phic, D.walls, D.walls_all, D.pout,
-                          D.Sp, D.ffi, D.rr_old, D.rr_new, (AT*)D.acc, D.status, D.tm_phi, D.tm_rinv, e.z0, e.y0,
+                          D.Sp, D.ffi, D.rr_old, D.rr_new, (AT*)D.acc, D.status, D.tm_phi, D.tm_ref, e.z0, e.y0,
                           e.xa, e.xb, sm, nload, D.solid != 0);
     __syncthreads();
   }
@@ -143,7 +143,7 @@ struct sym_batch {
   std::vector<int> built_cur, built_pc;   // domain parities graph 0 was built for
   int steps_since_build = 0;
   DomainDesc* d_desc[2] = {nullptr, nullptr};
-  CUtensorMap* d_tmaps = nullptr;   // [parity][domain][phase field, 1/rho_ref]
+  CUtensorMap* d_tmaps = nullptr;   // [parity][domain][phase field, reference pairs]
   int2* d_blk = nullptr;          // phase block -> (domain, block in domain)
   TileEntry* d_tiles = nullptr;
   int ntiles = 0;
@@ -289,9 +289,9 @@ int build(sym_batch* b) {
       const int pc = (b->built_pc[i] + k) & 1;
       const size_t j = ((size_t)k * n + i) * 2;
       maps[j] = b->doms[i]->fast.tm_phi[pc];
-      maps[j + 1] = b->doms[i]->fast.tm_rinv[pc];
+      maps[j + 1] = b->doms[i]->fast.tm_ref[pc];
       desc[k][i].tm_phi = b->d_tmaps + j;
-      desc[k][i].tm_rinv = b->d_tmaps + j + 1;
+      desc[k][i].tm_ref = b->d_tmaps + j + 1;
     }
   cudaMemcpyAsync(b->d_tmaps, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice, b->st);
   for (int k = 0; k < 2; k++) {

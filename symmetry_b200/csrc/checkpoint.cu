@@ -56,7 +56,7 @@ std::vector<Section> sections(sym_handle* h, bool fused) {
     s.push_back({"populations", F.pop[F.cur], 38 * N * sp});
     s.push_back({"phase_field", F.storage == SYM_STORE_FP64 ? (void*)F.phi[1 - F.pc] : (void*)F.phif[1 - F.pc],
                  phib});
-    if (F.storage == SYM_STORE_FP16) s.push_back({"ref_density", F.rref[1 - F.pc], sizeof(float) * pd.size()});
+    if (F.storage == SYM_STORE_FP16) s.push_back({"reference_pairs", F.rref[1 - F.pc], sizeof(float2) * pd.size()});
     if (F.acc) s.push_back({"accumulators", F.acc, 2 * N * 8});
     s.push_back({"status", F.status, sizeof(int)});
     if (h->dp.par > 0) s.push_back({"ffi", h->ffi, 19 * ND});   // held from creation
@@ -182,6 +182,10 @@ int sym_checkpoint_load(sym_handle* h, const char* path) {
     if (fread(buf.data(), 1, n, in.f) != n) return set_error(h, SYM_ERR_PARAM, "checkpoint: %s is truncated", path);
     void* dst = s.dev ? s.dev : (void*)h->dpart;
     if (int e = check_cuda(h, cudaMemcpy(dst, buf.data(), n, cudaMemcpyHostToDevice), "checkpoint write")) return e;
+  }
+  if (fused) {   // the momentum link lists follow from the restored masks
+    if (int e = sparse_links_build(h, h->st)) return set_error(h, e, "checkpoint: momentum link lists");
+    if (int e = check_cuda(h, cudaStreamSynchronize(h->st), "checkpoint links")) return e;
   }
   h->fast.valid = fused;
   return SYM_OK;

@@ -31,6 +31,7 @@
 #include <vector>
 #include "state.cuh"
 #include "fused.cuh"
+#include "particles.cuh"
 
 namespace symb200 {
 
@@ -54,8 +55,8 @@ float* phibuf<__half>(sym_handle* h, int k) { return h->fast.phif[k]; }
 
 // reference densities of the 16-bit storage: decoded with rr[1 - pc], written
 // by this step's phase kernel into rr[pc] (null for the other storages)
-const float* rr_old(const sym_handle* h, int pc) { return h->fast.rref[1 - pc]; }
-float* rr_new(sym_handle* h, int pc) { return h->fast.rref[pc]; }
+const float2* rr_old(const sym_handle* h, int pc) { return h->fast.rref[1 - pc]; }
+float2* rr_new(sym_handle* h, int pc) { return h->fast.rref[pc]; }
 
 bool has_solids(const sym_handle* h) { return h->dp.par > 0 || h->dp.wall_x; }
 
@@ -112,7 +113,7 @@ int enqueue_step(sym_handle* h, int cur, int pc, cudaEvent_t* ev) {
   dim3 grid((P.nz + BZ - 1) / BZ, (P.ny + BY - 1) / BY, (P.nx + xc - 1) / xc);
   const size_t shm = smem_bytes<S>();
   const CUtensorMap& tp = h->fast.tm_phi[pc];
-  const CUtensorMap& tr = h->fast.tm_rinv[pc];
+  const CUtensorMap& tr = h->fast.tm_ref[pc];
   if (ev) cudaEventRecord(ev[2], h->st);
   if (solid)
     k_collide<S, true><<<grid, TPB, shm, h->st>>>(P, pd, pin_, pnext, phic, h->walls, h->walls_all, h->pout,
@@ -190,14 +191,22 @@ int fast_alloc(sym_handle* h) {
       if (int e = dev_carve(h, (void**)&F.phif[k], sizeof(float) * pd.size())) return e;
     }
     if (F.storage == SYM_STORE_FP16)
-      if (int e = dev_carve(h, (void**)&F.rref[k], sizeof(float) * pd.size())) return e;
+      if (int e = dev_carve(h, (void**)&F.rref[k], sizeof(float2) * pd.size())) return e;
   }
   if (F.storage == SYM_STORE_FP64)   // the storage whose collide kernel accumulates (kAccumulate)
     if (int e = dev_carve(h, &F.acc, 2 * h->N * 8)) return e;
+  if (h->dp.par > 0) {
+    // momentum link lists: one 256-entry segment per block of each particle's
+    // momentum box (the box of set_walls' pin/pout marking)
+    F.link_blocks = (part::sphere_box(h->dp, part::kLinkMargin).count() + 255) / 256;
+    const size_t segs = (size_t)h->dp.par * F.link_blocks;
+    if (int e = dev_carve(h, (void**)&F.links, segs * 256 * sizeof(uint2))) return e;
+    if (int e = dev_carve(h, (void**)&F.nlinks, segs * sizeof(int))) return e;
+  }
   if (int e = dev_carve(h, (void**)&F.status, sizeof(int))) return e;
   if (h->planning) return SYM_OK;
   F.bytes = h->bytes - before;
-  // TMA descriptors of the phase-field (and 16-bit 1/rho_ref) tiles the
+  // TMA descriptors of the phase-field (and 16-bit reference-pair) tiles the
   // collide kernel reads: boxes of (BZ+4) x (BY+4) x 1 over the padded arrays
   for (int k = 0; k < 2; k++) {
     const bool f64 = F.storage == SYM_STORE_FP64;
@@ -205,10 +214,10 @@ int fast_alloc(sym_handle* h) {
     if (tma::encode_padded(&F.tm_phi[k], phi, f64 ? 8 : 4, h->dp.nz + 4, pd.nzp, pd.nyp, pd.nxp, BZ + 4, BY + 4))
       return set_error(h, SYM_ERR_CUDA, "TMA descriptor of the phase field");
     if (F.storage == SYM_STORE_FP16) {
-      if (tma::encode_padded(&F.tm_rinv[k], F.rref[k], 4, h->dp.nz + 4, pd.nzp, pd.nyp, pd.nxp, BZ + 4, BY + 4))
+      if (tma::encode_padded(&F.tm_ref[k], F.rref[k], 8, h->dp.nz + 4, pd.nzp, pd.nyp, pd.nxp, BZ + 4, BY + 4))
         return set_error(h, SYM_ERR_CUDA, "TMA descriptor of the reference densities");
     } else {
-      F.tm_rinv[k] = F.tm_phi[k];   // not read
+      F.tm_ref[k] = F.tm_phi[k];   // not read
     }
   }
   return F.storage == SYM_STORE_FP64 ? set_smem_attr<double>(h)
@@ -227,8 +236,12 @@ void fast_free(sym_handle* h) {
     if (k == 0) {
       dev_release(h, F.acc);
       dev_release(h, (void*)F.status);
+      dev_release(h, (void*)F.links);
+      dev_release(h, (void*)F.nlinks);
       F.acc = nullptr;
       F.status = nullptr;
+      F.links = nullptr;
+      F.nlinks = nullptr;
     }
     if (F.gexec[k]) cudaGraphExecDestroy(F.gexec[k]);
     if (F.graph[k]) cudaGraphDestroy(F.graph[k]);
@@ -263,6 +276,7 @@ int fast_import(sym_handle* h) {
                                                                 accbuf<__half>(h), F.status);
       k_import_phi<float><<<blocks_for(P.N), 256, 0, h->st>>>(P, pd, h->rhoN, F.phif[1]);
   }
+  if (int e = sparse_links_build(h, h->st)) return set_error(h, e, "momentum link lists");
   return check_cuda(h, cudaStreamSynchronize(h->st), "fast import");
 }
 

@@ -56,18 +56,28 @@ __device__ __forceinline__ void phi_store(const DevParams& P, const Pad& pd, R* 
 // Each velocity i holds an array of N slot pairs, pair index i*N + L: one
 // aligned 2-slot load or store per velocity (8/16-byte pairs, 4-byte for the
 // 16-bit storage), so a warp moves whole 128-byte lines per instruction.
-// FP64 / FP32: the pair is (r, b).  16-bit storage: the low half holds
-// q = 4096 (f/(w rho_ref) - 1) in FP16 -- the deviation of the total
-// population from the rest equilibrium w rho_ref of the node it is stored at,
-// with rho_ref that node's density of the step that wrote it (so the Laplace
-// pressure jump of a drop or thread does not eat the significand, and the
-// 2^12 scale keeps deviations down to 1e-8 out of the FP16 subnormal range)
-// -- and the high half the colour fraction c = r/f as 16-bit fixed point
-// k = 16384 + 32768 c over c in [-0.5, 1.5) (step 3.05e-5; the pure phases
-// c = 0 and c = 1 are the exact codes 16384 and 49152).
+// FP64 / FP32: the pair is (r, b).
+// 16-bit storage (shifted storage, FP32 arithmetic): the pair is two FP16
+// numbers relative to a reference pair (rho_ref, chi_ref) -- the density and
+// red fraction of the node the population is stored at, from the step that
+// wrote it (FP32):
+//   q = 4096 (f - w rho_ref) / w    the total's deviation from its rest
+//                                   equilibrium (the Laplace pressure jump
+//                                   does not eat the significand; the 2^12
+//                                   scale keeps deviations down to 1e-8 out
+//                                   of the FP16 subnormal range)
+//   d = r / f - chi_ref             the red fraction's deviation from the
+//                                   node's: exactly 0 in a pure phase, and the
+//                                   small colour perturbations that seed an
+//                                   instability keep FP16's 2^-11 relative
+//                                   precision instead of a fixed step
+// Encoder and decoder share the rounded rest equilibrium e = w rho_ref (one
+// product, never contracted), so the rounding of the scale factors multiplies
+// only the deviation and adds no bias to the mass.
 // Indices are 32-bit pair offsets (the fused path requires 38*N < 2^32).
-// load takes the node's rho_ref, store takes 1/rho_ref of the destination
-// node (only the 16-bit codec uses them; kRef says whether it does).
+// load and store take the reference pair of the node the population is
+// stored at (only the 16-bit codec uses it; kRef says whether it does).
+using Ref = float2;
 template <typename S>
 struct Codec;
 template <>
@@ -75,20 +85,21 @@ struct Codec<double> {
   using R = double;
   static constexpr bool kRef = false;
   template <int I>
-  __device__ __forceinline__ static void load(const double* __restrict__ p, unsigned N, unsigned L, R, R& r, R& b) {
+  __device__ __forceinline__ static void load(const double* __restrict__ p, unsigned N, unsigned L, Ref, R& r, R& b) {
     const double2 v = reinterpret_cast<const double2*>(p)[I * N + L];
     r = v.x;
     b = v.y;
   }
   // total f = r + b and red r
   template <int I>
-  __device__ __forceinline__ static void load_fr(const double* __restrict__ p, unsigned N, unsigned L, R, R& f, R& r) {
+  __device__ __forceinline__ static void load_fr(const double* __restrict__ p, unsigned N, unsigned L, Ref, R& f,
+                                                 R& r) {
     const double2 v = reinterpret_cast<const double2*>(p)[I * N + L];
     r = v.x;
     f = v.x + v.y;
   }
   template <int I>
-  __device__ __forceinline__ static void store(double* p, unsigned N, unsigned L, R, R r, R f) {
+  __device__ __forceinline__ static void store(double* p, unsigned N, unsigned L, Ref, R r, R f) {
     reinterpret_cast<double2*>(p)[I * N + L] = make_double2(r, f - r);
   }
 };
@@ -97,19 +108,20 @@ struct Codec<float> {
   using R = float;
   static constexpr bool kRef = false;
   template <int I>
-  __device__ __forceinline__ static void load(const float* __restrict__ p, unsigned N, unsigned L, R, R& r, R& b) {
+  __device__ __forceinline__ static void load(const float* __restrict__ p, unsigned N, unsigned L, Ref, R& r, R& b) {
     const float2 v = reinterpret_cast<const float2*>(p)[I * N + L];
     r = v.x;
     b = v.y;
   }
   template <int I>
-  __device__ __forceinline__ static void load_fr(const float* __restrict__ p, unsigned N, unsigned L, R, R& f, R& r) {
+  __device__ __forceinline__ static void load_fr(const float* __restrict__ p, unsigned N, unsigned L, Ref, R& f,
+                                                 R& r) {
     const float2 v = reinterpret_cast<const float2*>(p)[I * N + L];
     r = v.x;
     f = v.x + v.y;
   }
   template <int I>
-  __device__ __forceinline__ static void store(float* p, unsigned N, unsigned L, R, R r, R f) {
+  __device__ __forceinline__ static void store(float* p, unsigned N, unsigned L, Ref, R r, R f) {
     reinterpret_cast<float2*>(p)[I * N + L] = make_float2(r, f - r);
   }
 };
@@ -117,43 +129,39 @@ template <>
 struct Codec<__half> {
   using R = float;
   static constexpr bool kRef = true;
+  // total f and red r
   template <int I>
-  __device__ __forceinline__ static void load(const __half* __restrict__ p, unsigned N, unsigned L, R rref, R& r,
+  __device__ __forceinline__ static void load_fr(const __half* __restrict__ p, unsigned N, unsigned L, Ref ref, R& f,
+                                                 R& r) {
+    const float2 q = __half22float2(reinterpret_cast<const __half2*>(p)[I * N + L]);
+    f = fmaf(q.x, float(W(I) / 4096.0), __fmul_rn(float(W(I)), ref.x));
+    r = f * (ref.y + q.y);
+  }
+  template <int I>
+  __device__ __forceinline__ static void load(const __half* __restrict__ p, unsigned N, unsigned L, Ref ref, R& r,
                                               R& b) {
-    const unsigned w = reinterpret_cast<const unsigned*>(p)[I * N + L];
-    const R q = __half2float(__ushort_as_half((unsigned short)(w & 0xffffu)));
-    // the colour code k sits in the low mantissa bits of 2^23 + k, so it
-    // reaches FP32 without a conversion instruction; c = k/32768 - 1/2 exactly
-    const R kf = __uint_as_float(0x4B000000u | (w >> 16));
-    const R c = fmaf(kf, 1.0f / 32768.0f, -(8388608.0f + 16384.0f) / 32768.0f);
-    const R wr = R(W(I)) * rref;
-    const R f = fmaf(wr * (1.0f / 4096.0f), q, wr);
-    r = f * c;
+    R f;
+    load_fr<I>(p, N, L, ref, f, r);
     b = f - r;
   }
-  // the stored total f directly (and its red part): no b = f - r round trip
   template <int I>
-  __device__ __forceinline__ static void load_fr(const __half* __restrict__ p, unsigned N, unsigned L, R rref, R& f,
-                                                 R& r) {
-    const unsigned w = reinterpret_cast<const unsigned*>(p)[I * N + L];
-    const R q = __half2float(__ushort_as_half((unsigned short)(w & 0xffffu)));
-    const R kf = __uint_as_float(0x4B000000u | (w >> 16));
-    const R c = fmaf(kf, 1.0f / 32768.0f, -(8388608.0f + 16384.0f) / 32768.0f);
-    const R wr = R(W(I)) * rref;
-    f = fmaf(wr * (1.0f / 4096.0f), q, wr);
-    r = f * c;
-  }
-  template <int I>
-  __device__ __forceinline__ static void store(__half* p, unsigned N, unsigned L, R irref, R r, R f) {
-    const R q = f * (R(4096.0 / W(I)) * irref) - R(4096);
-    const R c = fminf(fmaxf(__fdividef(r, f), -0.5f), 1.4999694824f);   // codes 0..65535
-    // 2^23 + 16384 + 32768 c rounds to an integer whose low 16 bits are the
-    // code (nearest, ties to even): no float-to-integer conversion needed
-    const R kf = fmaf(c, 32768.0f, 8388608.0f + 16384.0f);
-    const unsigned lo = __half_as_ushort(__float2half_rn(q));
-    reinterpret_cast<unsigned*>(p)[I * N + L] = __byte_perm(lo, __float_as_uint(kf), 0x5410);
+  __device__ __forceinline__ static void store(__half* p, unsigned N, unsigned L, Ref ref, R r, R f) {
+    constexpr float c = float(4096.0 / W(I));   // 12288, 73728 or 147456: exact
+    const R q = (f - __fmul_rn(float(W(I)), ref.x)) * c;
+    // the pure phases exactly (r = f, r = 0), other fractions by the fast quotient
+    const R d = (r == f ? R(1) : (r == R(0) ? R(0) : __fdividef(r, f))) - ref.y;
+    reinterpret_cast<__half2*>(p)[I * N + L] = __floats2half2_rn(q, d);
   }
 };
+// the reference pair of node colour densities (sr, sb): density and red
+// fraction (a pure phase exactly 1 or 0)
+__device__ __forceinline__ Ref ref_pair(float sr, float sb) {
+  const float rho = sr + sb;
+  return make_float2(rho, sr / rho);
+}
+// the reference pair of a node with no populations of its own (solid): the
+// rest density, half red
+__device__ __forceinline__ Ref ref_rest(const DevParams& P) { return make_float2(float(P.rho0), 0.5f); }
 
 // ---- next-step colour densities accumulated by the collide kernel ----------------
 // The collide kernel of a step pushes every post-collision population to the
@@ -215,50 +223,62 @@ __device__ __forceinline__ void unroll19(F&& f) {
 // ---- calmacros (Source1.f90:770-831) on the fused state ---------------------------
 // Storages that do not accumulate: phi = (rhoR - rhoB) / rho from the node's
 // own post-stream populations; 0 on solid nodes.  16-bit storage decodes with
-// rr_old and records 1/rho in rr_new (as finalize_nodes below).
+// the reference pairs rr_old and records the node's (rho, red fraction) in rr_new:
+// the references this step's encoders use and the next step decodes with.
 template <typename S, bool SOLID>
 __device__ __forceinline__ void phase_node(const DevParams& P, const Pad& pd, const S* __restrict__ pops,
                                            typename Codec<S>::R* __restrict__ phi,
-                                           const int32_t* __restrict__ walls_all, const float* __restrict__ rr_old,
-                                           float* __restrict__ rr_new, long long L) {
+                                           const int32_t* __restrict__ walls_all, const Ref* __restrict__ rr_old,
+                                           Ref* __restrict__ rr_new, long long L) {
   using R = typename Codec<S>::R;
   if (L >= P.N) return;
   const unsigned Lu = (unsigned)L, q = Lu / (unsigned)P.nz;
   const int z = (int)(Lu - q * (unsigned)P.nz), x = (int)(q / (unsigned)P.ny), y = (int)(q - (unsigned)x * P.ny);
   R v = R(0);
-  R rho = R(P.rho0);
+  Ref nref = ref_rest(P);
   if (!(SOLID && walls_all[L] >= 1)) {
     const unsigned N = (unsigned)P.N;
-    const R rref = Codec<S>::kRef ? R(1) / R(rr_old[pd.idx(x, y, z)]) : R(P.rho0);
-    R sr = R(0), sf = R(0);
-    unroll19([&](auto ic) {
-      constexpr int i = decltype(ic)::value;
-      R f, r;
-      Codec<S>::template load_fr<i>(pops, N, Lu, rref, f, r);
-      sr = sr + r;
-      sf = sf + f;
-    });
-    rho = sf;
-    v = qdiv<R>(sr - (sf - sr), rho);
+    if constexpr (Codec<S>::kRef) {
+      const Ref ref = rr_old[pd.idx(x, y, z)];
+      R sr = R(0), sb = R(0);
+      unroll19([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        R r, b;
+        Codec<S>::template load<i>(pops, N, Lu, ref, r, b);
+        sr = sr + r;
+        sb = sb + b;
+      });
+      v = qdiv<R>(sr - sb, sr + sb);
+      nref = ref_pair(float(sr), float(sb));
+    } else {
+      R sr = R(0), sf = R(0);
+      unroll19([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        R f, r;
+        Codec<S>::template load_fr<i>(pops, N, Lu, Ref{}, f, r);
+        sr = sr + r;
+        sf = sf + f;
+      });
+      v = qdiv<R>(sr - (sf - sr), sf);
+    }
   }
   phi_store<R>(P, pd, phi, x, y, z, v);
-  if (Codec<S>::kRef) phi_store<float>(P, pd, rr_new, x, y, z, 1.0f / float(rho));
+  if constexpr (Codec<S>::kRef) phi_store<Ref>(P, pd, rr_new, x, y, z, nref);
 }
 
 template <typename S, bool SOLID>
 __global__ void __launch_bounds__(256) k_phase(DevParams P, Pad pd, const S* __restrict__ pops,
                                                typename Codec<S>::R* __restrict__ phi,
-                                               const int32_t* __restrict__ walls_all, const float* __restrict__ rr_old,
-                                               float* __restrict__ rr_new) {
+                                               const int32_t* __restrict__ walls_all, const Ref* __restrict__ rr_old,
+                                               Ref* __restrict__ rr_new) {
   phase_node<S, SOLID>(P, pd, pops, phi, walls_all, rr_old, rr_new, blockIdx.x * 256LL + threadIdx.x);
 }
 
 // From the accumulated colour densities (the steady-state phase field):
 // phi = (rhoR - rhoB) / rho on fluid nodes, 0 on solid nodes, written with its
 // periodic ghost images; the accumulators are cleared for the collide kernel
-// of this step.  16-bit storage also records 1/rho (1/rho0 on solid nodes) in
-// rr_new: the reference density this step's encoders use and the next step
-// decodes with (rr_new here, rr_old there: both hold 1/rho_ref).
+// of this step.  A storage with references (kRef) would also record the
+// node's (rho, red fraction) in rr_new, as phase_node does.
 // Nodes L0, L0 + 256, ..., L0 + 256 (NPT-1) per thread: every load of all of
 // them is issued before the first store, so a thread keeps 2 NPT accumulator
 // reads in flight (nothing waits on a store).
@@ -266,7 +286,7 @@ template <typename S, bool SOLID, int NPT>
 __device__ __forceinline__ void finalize_nodes(const DevParams& P, const Pad& pd,
                                                typename Acc<typename Codec<S>::R>::T* __restrict__ acc,
                                                typename Codec<S>::R* __restrict__ phi,
-                                               const int32_t* __restrict__ walls_all, float* __restrict__ rr_new,
+                                               const int32_t* __restrict__ walls_all, Ref* __restrict__ rr_new,
                                                const int* __restrict__ status, long long L0) {
   using R = typename Codec<S>::R;
   using A = Acc<R>;
@@ -295,14 +315,14 @@ __device__ __forceinline__ void finalize_nodes(const DevParams& P, const Pad& pd
     const int z = (int)(Lu - q * (unsigned)P.nz), x = (int)(q / (unsigned)P.ny), y = (int)(q - (unsigned)x * P.ny);
     const R sr = A::val(ar[k]), sb = A::val(ab[k]);
     R v = R(0);
-    R rho = R(P.rho0);
+    Ref nref = ref_rest(P);
     if (!solid[k]) {
-      rho = sr + sb;
-      v = qdiv<R>(sr - sb, rho);
+      v = qdiv<R>(sr - sb, sr + sb);
+      nref = ref_pair(float(sr), float(sb));
     }
     if (bad) v = R(NAN);
     phi_store<R>(P, pd, phi, x, y, z, v);
-    if (Codec<S>::kRef) phi_store<float>(P, pd, rr_new, x, y, z, 1.0f / float(rho));
+    if constexpr (Codec<S>::kRef) phi_store<Ref>(P, pd, rr_new, x, y, z, nref);
   }
 }
 
@@ -312,7 +332,7 @@ constexpr int kFinalizeNPT = 4;
 template <typename S, bool SOLID>
 __global__ void __launch_bounds__(256) k_finalize(DevParams P, Pad pd, typename Acc<typename Codec<S>::R>::T* acc,
                                                   typename Codec<S>::R* __restrict__ phi,
-                                                  const int32_t* __restrict__ walls_all, float* __restrict__ rr_new,
+                                                  const int32_t* __restrict__ walls_all, Ref* __restrict__ rr_new,
                                                   const int* __restrict__ status) {
   finalize_nodes<S, SOLID, kFinalizeNPT>(P, pd, acc, phi, walls_all, rr_new, status,
                                          blockIdx.x * (256LL * kFinalizeNPT) + threadIdx.x);
@@ -332,13 +352,13 @@ __device__ __forceinline__ void wet_rotate(const DevParams& P, const sym_particl
 }
 
 // ---- k_collide ------------------------------------------------------------------
-// phi ring of 5 planes, normal ring of 4 planes, 1/rho_ref ring of 6 planes:
-// normals are computed one plane ahead and phi / 1/rho_ref loaded three planes
+// phi ring of 5 planes, normal ring of 4 planes, reference-pair ring of 6 planes:
+// normals are computed one plane ahead and phi / reference-pair loaded three planes
 // ahead, before the plane's single barrier.  A warp that has finished plane x
 // runs those writes for plane x+1 while slower warps still read plane x's
-// slots: phi at x, normals at x-1..x+1 and 1/rho_ref at x-1..x+1 (the push
+// slots: phi at x, normals at x-1..x+1 and reference-pair at x-1..x+1 (the push
 // targets).  The rings are sized so that the slots written for plane x+1
-// (phi x+4 -> slot (x-1)%5, normals x+2 -> (x-2)%4, 1/rho_ref x+4 -> (x-2)%6)
+// (phi x+4 -> slot (x-1)%5, normals x+2 -> (x-2)%4, reference-pair x+4 -> (x-2)%6)
 // are never among them.
 constexpr int kIrrRing = 6;
 // unit normal and |grad phi| of one node, read with one (FP32) or two (FP64)
@@ -347,16 +367,16 @@ template <typename R>
 struct alignas(4 * sizeof(R)) NormalV {
   R x, y, z, g;
 };
-// phi and 1/rho_ref plane tiles ((BY+4) x (BZ+4), z fastest) arrive by TMA:
+// phi and reference-pair plane tiles ((BY+4) x (BZ+4), z fastest) arrive by TMA:
 // each slot starts on a 128-byte boundary
 constexpr int kPlaneTile = (BY + 4) * (BZ + 4);
 template <typename S>
 struct Smem {
   using R = typename Codec<S>::R;
   static constexpr int kPhiSlot = (kPlaneTile * (int)sizeof(R) + 127) / 128 * 128 / (int)sizeof(R);
-  static constexpr int kIrrSlot = (kPlaneTile * 4 + 127) / 128 * 128 / 4;
+  static constexpr int kRefSlot = (kPlaneTile * 8 + 127) / 128 * 128 / 8;
   alignas(128) R phi[5][kPhiSlot];
-  alignas(128) float irr[Codec<S>::kRef ? kIrrRing : 1][kIrrSlot];   // 1/rho_ref of this step (16-bit storage)
+  alignas(128) Ref ref[Codec<S>::kRef ? kIrrRing : 1][kRefSlot];   // reference pairs of this step (16-bit storage)
   NormalV<R> n[4][BY + 2][BZ + 2];   // [plane][y][z]: n and |grad phi|
   // [cx+1][to row y+1, y-1][colour]: density sums crossing rows (accumulating
   // storages only; a single element otherwise)
@@ -398,9 +418,9 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
                                              const int32_t* __restrict__ walls_all,
                                              const int32_t* __restrict__ pout,
                                              const sym_particles* __restrict__ Sp, double* __restrict__ ffi,
-                                             const float* __restrict__ rr_old, const float* __restrict__ rr_new,
+                                             const Ref* __restrict__ rr_old, const Ref* __restrict__ rr_new,
                                              typename Acc<typename Codec<S>::R>::T* acc, int* status,
-                                             const CUtensorMap* tm_phi, const CUtensorMap* tm_rinv,
+                                             const CUtensorMap* tm_phi, const CUtensorMap* tm_ref,
                                              int z0, int y0, int xa, int xb, Smem<S>& sm, unsigned& nload,
                                              bool solid_rt = true) {
   using R = typename Codec<S>::R;
@@ -411,24 +431,23 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
   constexpr bool REF = Codec<S>::kRef;
   const int tz = threadIdx.x % BZ, ty = threadIdx.x / BZ;
   const unsigned N = (unsigned)P.N;
-  const R irho0 = R(1.0 / P.rho0);
   const R evap = R(P.evap);
   const int sy = P.nz, sx = P.nz * P.ny;   // element strides of y and x
 
-  // phi (and 1/rho_ref) of plane xp by TMA: one box of (BY+4) x (BZ+4) at the
+  // phi (and the reference pairs) of plane xp by TMA: one box of (BY+4) x (BZ+4) at the
   // padded origin (z0, y0, xp+2) -- z0 is a multiple of 32 elements, so the
   // innermost coordinate is 128-byte aligned; rows past the padded extent read
   // as zeros.  Plane xp is load number nl0 + xp - (xa - 2) of this CTA, on
   // mbarrier (number mod 6) with phase parity (number / 6) mod 2.
   const unsigned nl0 = nload;
   auto load_no = [&](int xp) { return nl0 + (unsigned)(xp - (xa - 2)); };
-  constexpr uint32_t kTx = kPlaneTile * (sizeof(R) + (REF ? 4 : 0));
+  constexpr uint32_t kTx = kPlaneTile * (sizeof(R) + (REF ? sizeof(Ref) : 0));
   auto load_phi = [&](int xp) {   // thread 0 only
     const unsigned q = load_no(xp);
     uint64_t* bar = &sm.bar[q % kIrrRing];
     tma::mbar_expect_tx(bar, kTx);
     tma::load_3d(sm.phi[((xp % 5) + 5) % 5], tm_phi, z0, y0, xp + 2, bar);
-    if (REF) tma::load_3d(sm.irr[((xp % kIrrRing) + kIrrRing) % kIrrRing], tm_rinv, z0, y0, xp + 2, bar);
+    if (REF) tma::load_3d(sm.ref[(unsigned)(xp + kIrrRing) % kIrrRing], tm_ref, z0, y0, xp + 2, bar);
   };
   auto wait_phi = [&](int xp) {   // every thread
     const unsigned q = load_no(xp);
@@ -515,7 +534,7 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
   R aPr = R(0), aPb = R(0), aCr = R(0), aCb = R(0), aNr = R(0), aNb = R(0);   // planes x-1, x, x+1
   for (int x = xa; x < xb; x++) {
     // phi of plane x+3 on its way; normals of plane x+1 from phi planes x..x+2.
-    // The slots the load overwrites (phi of plane x-2, 1/rho_ref of plane x-3)
+    // The slots the load overwrites (phi of plane x-2, reference pairs of plane x-3)
     // were last read before the previous plane's barriers.
     if (threadIdx.x == 0 && x + 3 <= xb + 1) load_phi(x + 3);
     wait_phi(x + 2);
@@ -541,19 +560,28 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
     R sfr = R(0), sfb = R(0);
     // accumulating kernels run every lane of a warp with an active node (the
     // shuffles need the whole warp); the others skip inactive nodes
-    if (ACC ? __any_sync(0xffffffffu, act) : act) {
-    if (sizeof(R) == 8 && x + 1 < xb) {
-      // FP64: bring the next plane's populations toward L2 while this plane
-      // computes (the FP32-math kernels, bound by instruction issue, measured
-      // faster without the 19 prefetch instructions)
-#pragma unroll
-      for (int i = 0; i < 19; i++) asm volatile("prefetch.global.L2 [%0];" ::"l"(pin_ + 2 * (i * N + L + sx)));
+    if (sizeof(R) == 8 && x + 1 < xb && threadIdx.x < 19 * BY) {
+      // FP64: the next plane's populations toward L2 while this plane
+      // computes, one bulk prefetch per (velocity, row) of the tile, by
+      // 19 x BY threads; the range is widened to 16-byte boundaries inside
+      // the array.  (Measured: FP64 collide 4.71 ms with it, 4.87 with one
+      // prefetch per population and thread, 4.89 without on the C3 thread;
+      // the FP32-math kernels are faster without any.)
+      constexpr size_t PB = 2 * sizeof(S);   // bytes per slot pair
+      const int i = threadIdx.x / BY, yy = y0 + (int)threadIdx.x % BY;
+      if (yy < P.ny) {
+        const size_t a = ((size_t)i * N + (size_t)(z0 + sy * yy + sx * (x + 1))) * PB;
+        const size_t e = min(a + (size_t)min(BZ, P.nz - z0) * PB + 15, (size_t)19 * N * PB) & ~size_t(15);
+        const size_t b = a & ~size_t(15);
+        if (e > b) tma::prefetch_l2(reinterpret_cast<const char*>(pin_) + b, (uint32_t)(e - b));
+      }
     }
+    if (ACC ? __any_sync(0xffffffffu, act) : act) {
     // calmacros on the own populations
     // (rho_B = rho - rho_R: a pure colour stays exactly pure, as r = f there)
     R f[19];
     R sr = R(0), rho = R(0);
-    const R rref = REF ? R(1) / R(rr_old[pd.idx(x, yc, zc)]) : R(P.rho0);
+    const Ref rref = REF ? rr_old[pd.idx(x, yc, zc)] : Ref{};
     unroll19([&](auto ic) {
       constexpr int i = decltype(ic)::value;
       R r;
@@ -661,17 +689,17 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
             const R star = flat ? R(0) : uw0 * R(CX(j)) + uw1 * R(CY(j)) + uw2 * R(CZ(j));
             const R rr = r + R(6.0 * W(j)) * sr * star;
             const R bb = (f[i] - r) + R(6.0 * W(j)) * sb * star;
-            const R irr = REF ? R(sm.irr[(unsigned)x % kIrrRing][(ty + 2) * (BZ + 4) + tz + 2]) : irho0;
-            Codec<S>::template store<j>(pout_, N, L, irr, rr, rr + bb);
+            const Ref rd = REF ? sm.ref[(unsigned)x % kIrrRing][(ty + 2) * (BZ + 4) + tz + 2] : Ref{};
+            Codec<S>::template store<j>(pout_, N, L, rd, rr, rr + bb);
             sfr = sfr + rr;
             sfb = sfb + bb;
             return;
           }
         }
-        const R irr =
-            REF ? R(sm.irr[(unsigned)(x + CX(i) + kIrrRing) % kIrrRing][(ty + 2 + CY(i)) * (BZ + 4) + tz + 2 + CZ(i)])
-                : irho0;
-        Codec<S>::template store<i>(pout_, N, T, irr, r, f[i]);
+        const Ref rd = REF ? sm.ref[(unsigned)(x + CX(i) + kIrrRing) % kIrrRing]
+                                   [(ty + 2 + CY(i)) * (BZ + 4) + tz + 2 + CZ(i)]
+                           : Ref{};
+        Codec<S>::template store<i>(pout_, N, T, rd, r, f[i]);
         if constexpr (!ACC) return;
         const R bv = f[i] - r;
         const bool ext = (CX(i) > 0 && exp_) || (CX(i) < 0 && exm) || (CY(i) > 0 && eyp) || (CY(i) < 0 && eym) ||
@@ -760,17 +788,17 @@ __global__ void __launch_bounds__(TPB, collide_ctas<S>()) k_collide(DevParams P,
                                                    const int32_t* __restrict__ walls_all,
                                                    const int32_t* __restrict__ pout,
                                                    const sym_particles* __restrict__ Sp, double* __restrict__ ffi,
-                                                   const float* __restrict__ rr_old, const float* __restrict__ rr_new,
+                                                   const Ref* __restrict__ rr_old, const Ref* __restrict__ rr_new,
                                                    typename Acc<typename Codec<S>::R>::T* acc, int* status,
                                                    const __grid_constant__ CUtensorMap tm_phi,
-                                                   const __grid_constant__ CUtensorMap tm_rinv, int xchunk) {
+                                                   const __grid_constant__ CUtensorMap tm_ref, int xchunk) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   Smem<S>& sm = smem_view<S>(smem_raw);
   collide_init_barriers<S>(sm);
   unsigned nload = 0;
   const int xa = blockIdx.z * xchunk;
   collide_tile<S, SOLID>(P, pd, pin_, pout_, phi, walls, walls_all, pout, Sp, ffi, rr_old, rr_new, acc, status,
-                         &tm_phi, &tm_rinv, blockIdx.x * BZ, blockIdx.y * BY, xa, min(xa + xchunk, P.nx), sm, nload);
+                         &tm_phi, &tm_ref, blockIdx.x * BZ, blockIdx.y * BY, xa, min(xa + xchunk, P.nx), sm, nload);
 }
 
 // ---- the fused state's side of the particle and wall work ---------------------------
@@ -797,7 +825,7 @@ __device__ __forceinline__ void pinfill_node(const DevParams& P, const Pad& pd, 
 // particle box -- rho_N (this step's calmacros), rho_R/rho_B and fi (current
 // populations), and the previous step's gradient/normal (from the previous
 // pin-filled phi): what Lagrange_points, momentum and refilling read.
-// rr_old (16-bit storage): 1/rho_ref of the populations.
+// rr_old (16-bit storage): the reference pairs of the populations.
 template <typename S>
 __device__ __forceinline__ void prep_node(const DevParams& P, const Pad& pd, const sym_particles* __restrict__ Sp,
                                           const S* __restrict__ pops, const typename Codec<S>::R* __restrict__ phi_cur,
@@ -805,11 +833,11 @@ __device__ __forceinline__ void prep_node(const DevParams& P, const Pad& pd, con
                                           const int32_t* __restrict__ walls_all, const int32_t* __restrict__ pout,
                                           double* rhoN, double* rhoR, double* rhoB, double* fi, double* gx,
                                           double* gy, double* gz, double* nxv, double* nyv, double* nzv,
-                                          const float* __restrict__ rr_old, int x, int y, int z) {
+                                          const Ref* __restrict__ rr_old, int x, int y, int z) {
   using R = typename Codec<S>::R;
   const long long L = lin(P, x, y, z);
   const unsigned N = (unsigned)P.N;
-  const R rref = Codec<S>::kRef ? R(1) / R(rr_old[pd.idx(x, y, z)]) : R(P.rho0);
+  const Ref rref = Codec<S>::kRef ? rr_old[pd.idx(x, y, z)] : Ref{};
   if (walls_all[L] > 0) {
     rhoN[L] = 0.0;
     gx[L] = 0.0; gy[L] = 0.0; gz[L] = 0.0; nxv[L] = 0.0; nyv[L] = 0.0; nzv[L] = 0.0;
@@ -849,52 +877,59 @@ __device__ __forceinline__ void prep_node(const DevParams& P, const Pad& pd, con
 }
 
 // after refilling: a refilled node's canonical populations and phi into the
-// fused state (encoded with the reference this step's collide decodes with)
+// fused state, encoded with a reference pair of its own (its colour
+// densities), which it records in rr_old: the references this step's collide
+// decodes with
 template <typename S>
 __device__ __forceinline__ void refill_import_node(const DevParams& P, const Pad& pd, int pp, S* pops,
                                                    typename Codec<S>::R* phi_cur, const int32_t* __restrict__ pout,
                                                    const int32_t* __restrict__ walls_old,
                                                    const double* __restrict__ ri, const double* __restrict__ bi,
-                                                   const double* __restrict__ rhoN, const float* __restrict__ rr_old,
+                                                   const double* __restrict__ rhoN, Ref* __restrict__ rr_old,
                                                    int x, int y, int z) {
   using R = typename Codec<S>::R;
   const long long L = lin(P, x, y, z);
   const unsigned N = (unsigned)P.N;
   if (pout[L] != pp || walls_old[L] < 1) return;
-  const R irr = Codec<S>::kRef ? R(rr_old[pd.idx(x, y, z)]) : R(1.0 / P.rho0);
+  Ref ref{};
+  if constexpr (Codec<S>::kRef) {
+    double sr = 0.0, sb = 0.0;
+    for (int i = 0; i < 19; i++) { sr += ri[(size_t)i * N + L]; sb += bi[(size_t)i * N + L]; }
+    ref = sr + sb > 0.0 ? ref_pair(float(sr), float(sb)) : ref_rest(P);
+    phi_store<Ref>(P, pd, rr_old, x, y, z, ref);
+  }
   unroll19([&](auto ic) {
     constexpr int i = decltype(ic)::value;
     const R r = R(ri[(size_t)i * N + L]), b = R(bi[(size_t)i * N + L]);
-    Codec<S>::template store<i>(pops, N, (unsigned)L, irr, r, r + b);
+    Codec<S>::template store<i>(pops, N, (unsigned)L, ref, r, r + b);
   });
   phi_store<R>(P, pd, phi_cur, x, y, z, R(rhoN[L]));
 }
 
 // whole-domain conversions between the canonical arrays and the fused state
-// rr (16-bit storage, else null): receives each node's density, the
-// reference its populations are encoded with (a solid or empty node keeps rho0)
+// rr (16-bit storage, else null): receives each node's reference pair, its
+// colour densities (the rest pair where both are 0: solid or empty nodes)
 template <typename S>
 __global__ void k_import_pops(DevParams P, Pad pd, const double* __restrict__ ri, const double* __restrict__ bi,
-                              S* pops, float* rr, typename Acc<typename Codec<S>::R>::T* acc, int* status) {
+                              S* pops, Ref* rr, typename Acc<typename Codec<S>::R>::T* acc, int* status) {
   using R = typename Codec<S>::R;
   const long long L = blockIdx.x * 256LL + threadIdx.x;
   if (L >= P.N) return;
   const unsigned N = (unsigned)P.N;
-  R irr = R(1.0 / P.rho0);
+  Ref ref{};
   R sr = R(0), sb = R(0);
-  if (Codec<S>::kRef) {
-    double rho = 0.0;
-    for (int i = 0; i < 19; i++) rho += ri[(size_t)i * N + L] + bi[(size_t)i * N + L];
-    const float ref = rho > 0.0 ? float(rho) : float(P.rho0);
+  if constexpr (Codec<S>::kRef) {
+    double dr = 0.0, db = 0.0;
+    for (int i = 0; i < 19; i++) { dr += ri[(size_t)i * N + L]; db += bi[(size_t)i * N + L]; }
+    ref = dr + db > 0.0 ? ref_pair(float(dr), float(db)) : ref_rest(P);
     const unsigned Lu = (unsigned)L, q = Lu / (unsigned)P.nz;
     const int z = (int)(Lu - q * (unsigned)P.nz), x = (int)(q / (unsigned)P.ny), y = (int)(q - (unsigned)x * P.ny);
-    irr = R(1) / R(ref);
-    phi_store<float>(P, pd, rr, x, y, z, float(irr));
+    phi_store<Ref>(P, pd, rr, x, y, z, ref);
   }
   unroll19([&](auto ic) {
     constexpr int i = decltype(ic)::value;
     const R r = R(ri[(size_t)i * N + L]), b = R(bi[(size_t)i * N + L]);
-    Codec<S>::template store<i>(pops, N, (unsigned)L, irr, r, r + b);
+    Codec<S>::template store<i>(pops, N, (unsigned)L, ref, r, r + b);
     sr = sr + r;
     sb = sb + b;
   });
@@ -908,17 +943,17 @@ __global__ void k_import_pops(DevParams P, Pad pd, const double* __restrict__ ri
   }
 }
 template <typename S>
-__global__ void k_export_pops(DevParams P, Pad pd, const S* __restrict__ pops, const float* __restrict__ rr, double* ri,
+__global__ void k_export_pops(DevParams P, Pad pd, const S* __restrict__ pops, const Ref* __restrict__ rr, double* ri,
                               double* bi) {
   using R = typename Codec<S>::R;
   const long long L = blockIdx.x * 256LL + threadIdx.x;
   if (L >= P.N) return;
   const unsigned N = (unsigned)P.N;
-  R rref = R(P.rho0);
-  if (Codec<S>::kRef) {
+  Ref rref{};
+  if constexpr (Codec<S>::kRef) {
     const unsigned Lu = (unsigned)L, q = Lu / (unsigned)P.nz;
     const int z = (int)(Lu - q * (unsigned)P.nz), x = (int)(q / (unsigned)P.ny), y = (int)(q - (unsigned)x * P.ny);
-    rref = R(1) / R(rr[pd.idx(x, y, z)]);
+    rref = rr[pd.idx(x, y, z)];
   }
   unroll19([&](auto ic) {
     constexpr int i = decltype(ic)::value;
@@ -931,9 +966,9 @@ __global__ void k_export_pops(DevParams P, Pad pd, const S* __restrict__ pops, c
 // calmacros (Source1.f90:770-831) of the current fused populations without
 // touching the fused state: rho, u = sum f c / rho (no force shift) and
 // phi = (rhoR - rhoB) / rho on fluid nodes; phi = 0, u = 0, rho = rho0 on
-// solid nodes.  rr (16-bit storage): 1/rho_ref of the populations.
+// solid nodes.  rr (16-bit storage): the reference pairs of the populations.
 template <typename S>
-__global__ void k_macros(DevParams P, Pad pd, const S* __restrict__ pops, const float* __restrict__ rr,
+__global__ void k_macros(DevParams P, Pad pd, const S* __restrict__ pops, const Ref* __restrict__ rr,
                          const int32_t* __restrict__ walls_all, double* rho, double* ux, double* uy, double* uz,
                          double* rhoN) {
   using R = typename Codec<S>::R;
@@ -944,11 +979,11 @@ __global__ void k_macros(DevParams P, Pad pd, const S* __restrict__ pops, const 
     return;
   }
   const unsigned N = (unsigned)P.N;
-  R rref = R(P.rho0);
-  if (Codec<S>::kRef) {
+  Ref rref{};
+  if constexpr (Codec<S>::kRef) {
     const unsigned Lu = (unsigned)L, q = Lu / (unsigned)P.nz;
     const int z = (int)(Lu - q * (unsigned)P.nz), x = (int)(q / (unsigned)P.ny), y = (int)(q - (unsigned)x * P.ny);
-    rref = R(1) / R(rr[pd.idx(x, y, z)]);
+    rref = rr[pd.idx(x, y, z)];
   }
   double sr = 0.0, sb = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
   unroll19([&](auto ic) {

@@ -321,14 +321,6 @@ __device__ __forceinline__ void mrt_collide_pairs(const DevParams& P, R f[19], R
     if constexpr (MCONS(k)) m[k] = meq[k] + R(0.5) * fk[k];
     else m[k] = m[k] - s[k] * (m[k] - meq[k]) + (R(1) - R(0.5) * s[k]) * fk[k];
   });
-  {
-    R e = R(0);
-    static_for<19>([&](auto rc) {
-      constexpr int r = decltype(rc)::value;
-      if constexpr (MEVEN(r) && MINV(0, r) != 0.0) e = e + R(MINV(0, r)) * m[r];
-    });
-    f[0] = e;
-  }
   static_for<9>([&](auto kc) {
     constexpr int i = PREP(decltype(kc)::value);
     R e = R(0), o = R(0);
@@ -342,6 +334,24 @@ __device__ __forceinline__ void mrt_collide_pairs(const DevParams& P, R f[19], R
     f[i] = e + o;
     f[OPC(i)] = e - o;
   });
+  if constexpr (sizeof(R) == 4) {
+    // FP32 arithmetic: the rest population closes the mass balance, so the
+    // post-collision populations sum to rho up to the rounding of these
+    // additions.  The rounded inverse-transform coefficients would otherwise
+    // bias every node's mass the same way, step after step (a drift of about
+    // 1e-9 per step).
+    R s = R(0);
+#pragma unroll
+    for (int i = 1; i < 19; i++) s = s + f[i];
+    f[0] = rho - s;
+  } else {
+    R e = R(0);
+    static_for<19>([&](auto rc) {
+      constexpr int r = decltype(rc)::value;
+      if constexpr (MEVEN(r) && MINV(0, r) != 0.0) e = e + R(MINV(0, r)) * m[r];
+    });
+    f[0] = e;
+  }
 }
 
 // Link fraction of curve2 (Source1.f90:1055-1070): node at displacement

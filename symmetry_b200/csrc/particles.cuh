@@ -119,6 +119,15 @@ __device__ __forceinline__ int lag_idx(const DevParams& P, long long c, int n, i
   return (int)i;
 }
 
+// sin and cos of the two angles of Lagrange point `num` (:1826-1830): they
+// depend on the point index only, so a step can read them from a table
+__device__ __forceinline__ void lagrange_trig(const DevParams& P, int num, double& sa, double& ca, double& sb,
+                                              double& cb) {
+  const int na = num / (P.la_n + 1) + 1, nb = num % (P.la_n + 1) + 1;
+  const double aa = (double)(na - 1) * P.alpha, bb = (double)(nb - 1) * P.alpha;
+  sa = sin(aa); ca = cos(aa); sb = sin(bb); cb = cos(bb);
+}
+
 // Lagrange point `num` of particle pp: position, area element, interpolated
 // phase, flag and rotated normal
 __device__ __forceinline__ void lagrange_point(const DevParams& P, const sym_particles* __restrict__ S,
@@ -128,22 +137,28 @@ __device__ __forceinline__ void lagrange_point(const DevParams& P, const sym_par
                                                const double* __restrict__ nyv, const double* __restrict__ nzv,
                                                double* Lax, double* Lay, double* Laz, double* La_rhoN, double* La_nx,
                                                double* La_ny, double* La_nz, int32_t* La_flag, double* ds, int num,
-                                               int pp) {
+                                               int pp, const double* __restrict__ tab = nullptr) {
   const int EX[8] = {0, 1, 1, 0, 0, 1, 1, 0};
   const int EY[8] = {0, 0, 1, 1, 0, 0, 1, 1};
   const int EZ[8] = {0, 0, 0, 0, 1, 1, 1, 1};
   const int par = P.par;
   if (num >= P.la_num) return;
   const long long q = (long long)num * par + (pp - 1);
-  const int na = num / (P.la_n + 1) + 1, nb = num % (P.la_n + 1) + 1;
   const double cx = PC(S->center, par, pp, 0), cy = PC(S->center, par, pp, 1), cz = PC(S->center, par, pp, 2);
   const double Rad = P.rad, alpha = P.alpha;
-  const double aa = (double)(na - 1) * alpha, bb = (double)(nb - 1) * alpha;
-  const double lx = cx + Rad * sin(bb) * cos(aa);
-  const double ly = cy + Rad * sin(bb) * sin(aa);
-  const double lz = cz + Rad * cos(bb);
+  // the point's angles: from the table of sin/cos per point (lagrange_trig)
+  // when given, else computed here -- the same values either way
+  double sa, ca, sb, cb;
+  if (tab) {
+    sa = tab[4LL * num]; ca = tab[4LL * num + 1]; sb = tab[4LL * num + 2]; cb = tab[4LL * num + 3];
+  } else {
+    lagrange_trig(P, num, sa, ca, sb, cb);
+  }
+  const double lx = cx + Rad * sb * ca;
+  const double ly = cy + Rad * sb * sa;
+  const double lz = cz + Rad * cb;
   Lax[q] = lx; Lay[q] = ly; Laz[q] = lz;
-  ds[q] = Rad * Rad * sin(bb) * (alpha * alpha);
+  ds[q] = Rad * Rad * sb * (alpha * alpha);
   const bool in_domain = P.ref ? (lx < P.nx - 0.5 && ly >= 1.5 && ly < P.ny - 0.5 && lz < P.nz - 0.5) : true;
   double v = 0.0;
   int fl = 0;
@@ -323,6 +338,103 @@ __device__ __forceinline__ void momentum_final_body(const DevParams& P, sym_part
       if (k < 3) S->fp[k * par + pp - 1] = s;
       else S->tp[(k - 3) * par + pp - 1] = s;
     }
+  }
+}
+
+// ---- momentum over link lists (fused and batched paths) ------------------------
+// margin of the momentum box and of set_walls' pin/pout box (the same box)
+constexpr double kLinkMargin = 3.0;
+// The links of particle pp -- (fluid node, velocity i) with the node's
+// neighbour x - c_i inside the particle -- are kept per block of pp's
+// momentum box as a compact list: block b's entries are (node, 18-bit mask of
+// its links into pp) of the nodes of that block that have any, in thread
+// order, so the list and the sums over it are deterministic.  set_walls
+// rebuilds the lists of a step while it marks pin/pout (walls, and so the
+// links, change only there); the next step's momentum reads them.
+
+// the links of fluid node (x,y,z) into solid id: bit i set when the
+// neighbour x + c_i belongs to id
+__device__ __forceinline__ unsigned link_mask(const DevParams& P, int x, int y, int z, int id,
+                                              const int32_t* __restrict__ walls) {
+  unsigned m = 0;
+#pragma unroll
+  for (int i = 1; i < 19; i++) {
+    const long long nb = lin(P, wrapi(x + CX(i), P.nx), wrapi(y + CY(i), P.ny), wrapi(z + CZ(i), P.nz));
+    if (walls[nb] == id) m |= 1u << i;
+  }
+  return m;
+}
+
+// block-wide compaction of (L, mask) for the threads with has = true into
+// seg[0 .. count), in thread order; every thread of the block calls it
+__device__ __forceinline__ void link_compact(bool has, unsigned L, unsigned mask, uint2* seg, int* count,
+                                             int* sh /* [8] */) {
+  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const unsigned bal = __ballot_sync(0xffffffffu, has);
+  if (lane == 0) sh[warp] = __popc(bal);
+  __syncthreads();
+  int off = 0, tot = 0;
+  for (int w = 0; w < 8; w++) {
+    if (w < (int)warp) off += sh[w];
+    tot += sh[w];
+  }
+  if (has) seg[off + __popc(bal & ((1u << lane) - 1u))] = make_uint2(L, mask);
+  if (threadIdx.x == 0) *count = tot;
+  __syncthreads();
+}
+
+// one block of pp's links: the momentum exchange of its entries (the terms of
+// :1193-1259), reduced by warp shuffles and then over the block's 8 warps in
+// a fixed order into part[pp-1][blk]
+__device__ __forceinline__ void momentum_links_partial(const DevParams& P, int pp, const sym_particles* __restrict__ S,
+                                                       const int32_t* __restrict__ pout,
+                                                       const double* __restrict__ fi,
+                                                       const double* __restrict__ ffi, const uint2* __restrict__ seg,
+                                                       int count, double* part, long long nblk, long long blk,
+                                                       double* sh /* [8][6] */) {
+  const int par = P.par;
+  double a[6] = {0, 0, 0, 0, 0, 0};
+  if ((int)threadIdx.x < count) {
+    const uint2 e = seg[threadIdx.x];
+    const long long L = e.x, N = P.N;
+    if (pout[L] == pp) {   // a later particle's set_walls may have taken the node
+      const unsigned q = (unsigned)e.x / (unsigned)P.nz;
+      const int z = (int)(e.x - q * (unsigned)P.nz), x = (int)(q / (unsigned)P.ny), y = (int)(q - (unsigned)x * P.ny);
+      const double xr = disp(P, (double)(x + P.origin), PC(S->center, par, pp, 0), 0);
+      const double yr = disp(P, (double)(y + P.origin), PC(S->center, par, pp, 1), 1);
+      const double zr = disp(P, (double)(z + P.origin), PC(S->center, par, pp, 2), 2);
+      const double uw0 = PC(S->up, par, pp, 0) + zr * PC(S->rp, par, pp, 1) - yr * PC(S->rp, par, pp, 2);
+      const double uw1 = PC(S->up, par, pp, 1) + xr * PC(S->rp, par, pp, 2) - zr * PC(S->rp, par, pp, 0);
+      const double uw2 = PC(S->up, par, pp, 2) + yr * PC(S->rp, par, pp, 0) - xr * PC(S->rp, par, pp, 1);
+#pragma unroll
+      for (int i = 1; i < 19; i++) {
+        // the reference's link i (neighbour x - c_i inside, :1193-1203) is
+        // bit OPC(i) of the mask; i ascending as there
+        if (!(e.y >> OPC(i) & 1u)) continue;
+        const int j = OPC(i);
+        const double f = fi[i * N + L], g = ffi[j * N + L];
+        const double fmx = ((double)CX(i) - uw0) * f - ((double)CX(j) - uw0) * g;
+        const double fmy = ((double)CY(i) - uw1) * f - ((double)CY(j) - uw1) * g;
+        const double fmz = ((double)CZ(i) - uw2) * f - ((double)CZ(j) - uw2) * g;
+        a[0] = a[0] - fmx; a[1] = a[1] - fmy; a[2] = a[2] - fmz;
+        a[3] = a[3] - (yr * fmz - zr * fmy);
+        a[4] = a[4] - (zr * fmx - xr * fmz);
+        a[5] = a[5] - (xr * fmy - yr * fmx);
+      }
+    }
+  }
+  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int c = 0; c < 6; c++) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a[c] += __shfl_down_sync(0xffffffffu, a[c], o);
+    if (lane == 0) sh[warp * 6 + c] = a[c];
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    double v = 0.0;
+    for (int w = 0; w < 8; w++) v += sh[w * 6 + threadIdx.x];
+    part[((long long)(pp - 1) * nblk + blk) * 6 + threadIdx.x] = v;
   }
 }
 

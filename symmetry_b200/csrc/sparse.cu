@@ -10,11 +10,13 @@
 //   lagrange        Lagrange points (Lagrange_points :1799-1978)
 //   capillary       immersed area and capillary force, fixed-order partials
 //                   (:1864-1866, capillary_force2 :1980-2028), then the sums
-//   momentum        momentum exchange partials, then the sums (:1178-1261)
+//   momentum        momentum exchange over the link lists (warp-shuffle
+//                   partials per box block), then the sums (:1178-1261)
 //   move            repulsion and Newton-Euler, one thread per domain
 //                   (:1594-1671, :1263-1349)
 //   set_walls       masks (:326-395): reset on the previous box, flat wall
-//                   planes, sphere marks, pin/pout
+//                   planes, sphere marks, pin/pout and the link lists of the
+//                   next step's momentum
 //   refilling       uncovered nodes (:1351-1418), then into the fused state
 //   pin fill        fictitious phi on solid nodes next to fluid
 // and, after the collide kernel, with the interpolated bounce-back:
@@ -22,7 +24,9 @@
 //                   (:1036-1101)
 // Masks, refills and sums are written per particle in the same order as the
 // per-handle kernels of particles.cu, so results are those of the drop-in
-// path bit for bit.
+// path bit for bit -- except the momentum sums, which add the same per-node
+// terms in another order (over the links instead of a box-wide tree): equal
+// to rounding.
 #include <algorithm>
 #include <cstring>
 #include <string>
@@ -53,10 +57,14 @@ struct SpDom {
   void* pops;            // fused populations of this step
   void* phic;            // this step's phase field (pin-filled below)
   void* phip;            // the previous step's phase field
-  const float* rr_old;   // 16-bit storage: 1/rho_ref of the populations
+  Ref* rr_old;           // 16-bit storage: reference pairs of the populations
   void* pnext;           // the populations this step's collide kernel writes
-  const float* rr_cur;   // 16-bit storage: 1/rho_ref they are encoded with
+  const Ref* rr_cur;     // 16-bit storage: reference pairs they are encoded with
   void* acc;             // next step's accumulated colour densities
+  const double* ltab;    // sin/cos of each Lagrange point's angles (4 per point)
+  uint2* links;          // momentum link lists [particle][box block][kT] and their counts
+  int* nlinks;
+  long long link_blocks;
   int* status;
   Box bprep, bmom, bmark, bpin, bref, bpfill;
   long long nblk_mom;
@@ -86,7 +94,18 @@ __global__ void __launch_bounds__(kT) k_sp_lagrange(const SpDom* __restrict__ do
   const Blk e = map[blockIdx.x];
   const SpDom& D = doms[e.d];
   part::lagrange_point(D.P, D.S, D.walls, D.rhoN, D.gx, D.gy, D.gz, D.nx, D.ny, D.nz, D.lax, D.lay, D.laz, D.larhon,
-                       D.lanx, D.lany, D.lanz, D.laflag, D.lads, e.b * kT + threadIdx.x, e.pp);
+                       D.lanx, D.lany, D.lanz, D.laflag, D.lads, e.b * kT + threadIdx.x, e.pp, D.ltab);
+}
+
+// the Lagrange points' sin/cos table of a domain, once per plan
+__global__ void __launch_bounds__(kT) k_sp_lagrange_table(const SpDom* __restrict__ doms,
+                                                           const Blk* __restrict__ map) {
+  const Blk e = map[blockIdx.x];
+  const SpDom& D = doms[e.d];
+  const int num = e.b * kT + threadIdx.x;
+  if (num >= D.P.la_num) return;
+  double* t = const_cast<double*>(D.ltab) + 4LL * num;
+  part::lagrange_trig(D.P, num, t[0], t[1], t[2], t[3]);
 }
 
 __global__ void __launch_bounds__(kT) k_sp_capillary(const SpDom* __restrict__ doms, const Blk* __restrict__ map) {
@@ -105,11 +124,15 @@ __global__ void k_sp_capillary_final(const SpDom* __restrict__ doms, const Blk* 
   part::capillary_final_body(D.P, D.S, D.red, 1, 1, e.pp, threadIdx.x);
 }
 
+// momentum exchange over the link list of one block of the particle's box
+// (written by the previous step's set_walls, or by the import)
 __global__ void __launch_bounds__(kT) k_sp_momentum(const SpDom* __restrict__ doms, const Blk* __restrict__ map) {
-  __shared__ double sh[kT];
+  __shared__ double sh[8 * 6];
   const Blk e = map[blockIdx.x];
   const SpDom& D = doms[e.d];
-  part::momentum_partial(D.P, D.bmom, e.pp, D.S, D.walls, D.pout, D.fi, D.ffi, D.red, D.nblk_mom, e.b, sh);
+  const long long seg = (long long)(e.pp - 1) * D.link_blocks + e.b;
+  part::momentum_links_partial(D.P, e.pp, D.S, D.pout, D.fi, D.ffi, D.links + seg * kT, D.nlinks[seg], D.red,
+                               D.nblk_mom, e.b, sh);
 }
 
 __global__ void __launch_bounds__(kT) k_sp_momentum_final(const SpDom* __restrict__ doms,
@@ -179,12 +202,49 @@ __global__ void __launch_bounds__(kT) k_sp_pin_plane(const SpDom* __restrict__ d
   part::pinpout_node(D.P, xp, t / D.P.nz, t % D.P.nz, id, D.walls, D.walls_all, D.pin, D.pout);
 }
 
+// pin/pout of particle pp on one block of its box, and that block's link list
+// for the next step's momentum (every thread takes part in the compaction)
 __global__ void __launch_bounds__(kT) k_sp_pin_box(const SpDom* __restrict__ doms, const Blk* __restrict__ map) {
+  __shared__ int sh[8];
   const Blk e = map[blockIdx.x];
   const SpDom& D = doms[e.d];
   int x, y, z;
-  if (!part::box_node(D.P, D.bpin, D.S->center, e.pp, (long long)e.b * kT + threadIdx.x, x, y, z)) return;
-  part::pinpout_node(D.P, x, y, z, e.pp, D.walls, D.walls_all, D.pin, D.pout);
+  bool has = false;
+  unsigned L = 0, mask = 0;
+  if (part::box_node(D.P, D.bpin, D.S->center, e.pp, (long long)e.b * kT + threadIdx.x, x, y, z) &&
+      part::in_range(D.P, x, y, z)) {
+    part::pinpout_node(D.P, x, y, z, e.pp, D.walls, D.walls_all, D.pin, D.pout);
+    const long long l = lin(D.P, x, y, z);
+    if (D.walls_all[l] == 0) {
+      mask = part::link_mask(D.P, x, y, z, e.pp, D.walls);
+      has = mask != 0;
+      L = (unsigned)l;
+    }
+  }
+  const long long seg = (long long)(e.pp - 1) * D.link_blocks + e.b;
+  part::link_compact(has, L, mask, D.links + seg * kT, D.nlinks + seg, sh);
+}
+
+// the link lists of particle pp from the current masks (after an import)
+__global__ void __launch_bounds__(kT) k_links_build(DevParams P, part::Box b, int pp, const sym_particles* S,
+                                                    const int32_t* __restrict__ walls,
+                                                    const int32_t* __restrict__ walls_all, uint2* links,
+                                                    int* nlinks, long long link_blocks) {
+  __shared__ int sh[8];
+  int x, y, z;
+  bool has = false;
+  unsigned L = 0, mask = 0;
+  if (part::box_node(P, b, S->center, pp, (long long)blockIdx.x * kT + threadIdx.x, x, y, z) &&
+      part::in_range(P, x, y, z)) {
+    const long long l = lin(P, x, y, z);
+    if (walls_all[l] == 0) {
+      mask = part::link_mask(P, x, y, z, pp, walls);
+      has = mask != 0;
+      L = (unsigned)l;
+    }
+  }
+  const long long seg = (long long)(pp - 1) * link_blocks + blockIdx.x;
+  part::link_compact(has, L, mask, links + seg * kT, nlinks + seg, sh);
 }
 
 __global__ void __launch_bounds__(kT) k_sp_refill(const SpDom* __restrict__ doms, const Blk* __restrict__ map) {
@@ -251,8 +311,7 @@ __global__ void __launch_bounds__(kT) k_sp_curve2(const SpDom* __restrict__ doms
   const unsigned N = (unsigned)P.N;
   const double* ff = D.ffi;
   const double* rp = D.ffi + 19 * (size_t)N;
-  const R irr = Codec<S>::kRef ? R(D.rr_cur[D.pd.idx(x, y, z)]) : R(1.0 / P.rho0);
-  const R rref = Codec<S>::kRef ? R(1) / irr : R(P.rho0);
+  const Ref rref = Codec<S>::kRef ? D.rr_cur[D.pd.idx(x, y, z)] : Ref{};
   S* pops = (S*)D.pnext;
   const double* c = D.S->center;
   const double x0 = disp(P, (double)(x + P.origin), c[0 * par + pp - 1], 0);
@@ -283,7 +342,7 @@ __global__ void __launch_bounds__(kT) k_sp_curve2(const SpDom* __restrict__ doms
     Codec<S>::template load<i>(pops, N, (unsigned)L, rref, hr, hb);
     const double vr = 1.0 / (1.0 + qq) * (qq * (ar + br) + (1.0 - qq) * (double)cr + 6.0 * W(i) * rhoR * star);
     const double vb = 1.0 / (1.0 + qq) * (qq * (ab + bb) + (1.0 - qq) * (double)cb + 6.0 * W(i) * rhoB * star);
-    Codec<S>::template store<i>(pops, N, (unsigned)L, irr, R(vr), R(vr) + R(vb));
+    Codec<S>::template store<i>(pops, N, (unsigned)L, rref, R(vr), R(vr) + R(vb));
     dr += vr - (double)hr;
     db += vb - (double)hb;
   });
@@ -312,6 +371,7 @@ struct SparsePlan {
   Table fix[NFIX];
   std::vector<Table> mark, pin, refill;   // [particle index - 1]
   int* d_move = nullptr;   // domains with particles
+  double* d_ltab = nullptr;   // Lagrange sin/cos tables of every domain with particles
   int nmove = 0;
   int launches = 0;
 };
@@ -352,10 +412,13 @@ SpDom make_dom(sym_handle* h, int cur, int pc) {
   d.rr_cur = h->fast.rref[pc];
   d.acc = h->fast.acc;
   d.status = h->fast.status;
+  d.links = h->fast.links;
+  d.nlinks = h->fast.nlinks;
+  d.link_blocks = h->fast.link_blocks;
   d.bprep = part::sphere_box(h->dp, 6.0);
-  d.bmom = part::sphere_box(h->dp, 3.0);
+  d.bmom = part::sphere_box(h->dp, part::kLinkMargin);
   d.bmark = part::sphere_box(h->dp, 1.0);
-  d.bpin = part::sphere_box(h->dp, 3.0);
+  d.bpin = part::sphere_box(h->dp, part::kLinkMargin);
   d.bref = part::sphere_box(h->dp, 4.0);
   d.bpfill = part::sphere_box(h->dp, 2.0);
   d.nblk_mom = nblocks(d.bmom.count());
@@ -375,7 +438,20 @@ void sparse_plan_free(SparsePlan* p) {
     for (auto& t : *v)
       if (t.d) cudaFree(t.d);
   if (p->d_move) cudaFree(p->d_move);
+  if (p->d_ltab) cudaFree(p->d_ltab);
   delete p;
+}
+
+// The momentum link lists of a handle's particles from its current masks
+// (the fused state was just built from the canonical one), enqueued on st.
+int sparse_links_build(sym_handle* h, cudaStream_t st) {
+  const DevParams& P = h->dp;
+  if (P.par <= 0 || !h->fast.links) return SYM_OK;
+  const part::Box b = part::sphere_box(P, part::kLinkMargin);
+  for (int pp = 1; pp <= P.par; pp++)
+    k_links_build<<<(unsigned)h->fast.link_blocks, kT, 0, st>>>(P, b, pp, h->dpart, h->walls, h->walls_all,
+                                                                h->fast.links, h->fast.nlinks, h->fast.link_blocks);
+  return cudaGetLastError() == cudaSuccess ? SYM_OK : SYM_ERR_CUDA;
 }
 
 // Plan of the sparse work of `doms` (each at buffer parity cur0/pc0 for step
@@ -388,6 +464,9 @@ SparsePlan* sparse_plan_build(const std::vector<sym_handle*>& doms, const std::v
   if (n) p->storage = doms[0]->fast.storage;
   std::vector<SpDom> dd[2];
   std::vector<Blk> tb[SparsePlan::NFIX];
+  std::vector<Blk> ltb;            // blocks of the one-time Lagrange table launch
+  std::vector<long long> ltoff;    // each domain's table offset (doubles), -1 without particles
+  long long ltlen = 0;
   int maxpar = 0;
   std::vector<int> move;
   for (int i = 0; i < n; i++) {
@@ -399,7 +478,10 @@ SparsePlan* sparse_plan_build(const std::vector<sym_handle*>& doms, const std::v
     if (P.wall_x)
       for (int v = 0; v < 2; v++)
         for (int b = 0; b < plane_blk; b++) tb[SparsePlan::PFPLANE].push_back({i, 0, b, v});
+    ltoff.push_back(P.par > 0 ? ltlen : -1);
     if (P.par <= 0) continue;
+    for (long long b = 0; b < nblocks(P.la_num); b++) ltb.push_back({i, 0, (int)b, 0});
+    ltlen += 4LL * P.la_num;
     maxpar = std::max(maxpar, P.par);
     move.push_back(i);
     if (P.wall_x) {
@@ -434,6 +516,16 @@ SparsePlan* sparse_plan_build(const std::vector<sym_handle*>& doms, const std::v
     }
   }
   int e = SYM_OK;
+  if (ltlen > 0) {
+    if (cudaMalloc(&p->d_ltab, sizeof(double) * ltlen) != cudaSuccess) {
+      (void)cudaGetLastError();
+      e = SYM_ERR_OOM;
+    } else {
+      for (int k = 0; k < 2; k++)
+        for (int i = 0; i < n; i++)
+          if (ltoff[i] >= 0) dd[k][i].ltab = p->d_ltab + ltoff[i];
+    }
+  }
   for (int k = 0; k < 2 && !e && n; k++) {
     if (cudaMalloc(&p->d_dom[k], sizeof(SpDom) * n) != cudaSuccess) {
       (void)cudaGetLastError();
@@ -460,7 +552,13 @@ SparsePlan* sparse_plan_build(const std::vector<sym_handle*>& doms, const std::v
       cudaMemcpyAsync(p->d_move, move.data(), sizeof(int) * move.size(), cudaMemcpyHostToDevice, st);
     }
   }
+  SparsePlan::Table lt;
+  if (!e && !ltb.empty()) {
+    e = plan_table(lt, ltb, st);
+    if (!e) k_sp_lagrange_table<<<(unsigned)lt.n, kT, 0, st>>>(p->d_dom[0], lt.d);
+  }
   if (!e && cudaStreamSynchronize(st) != cudaSuccess) e = SYM_ERR_CUDA;
+  if (lt.d) cudaFree(lt.d);
   if (e) {
     *err = e;
     sparse_plan_free(p);

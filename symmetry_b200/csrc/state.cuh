@@ -22,13 +22,16 @@ struct FastState {
   int xchunk = 0;          // x planes per tile of the fused collide kernel (0 = default)
   double* phi[2] = {nullptr, nullptr};  // FP64 halo-padded phase field (pin-filled)
   float* phif[2] = {nullptr, nullptr};  // FP32 halo-padded phase field for FP32/FP16 storage
-  float* rref[2] = {nullptr, nullptr};  // 16-bit storage: halo-padded 1/rho_ref (same parity as phi)
+  float2* rref[2] = {nullptr, nullptr};  // 16-bit storage: halo-padded reference pairs (rho, red fraction), same parity as phi
   void* acc = nullptr;     // next step's colour densities, fixed point [red N][blue N] (see fused.cuh)
+  uint2* links = nullptr;  // particles: momentum link lists [particle][box block][256] (see particles.cuh)
+  int* nlinks = nullptr;   // entries of each [particle][box block]
+  long long link_blocks = 0;   // blocks of one particle's momentum box
   int* status = nullptr;   // sticky: bit 0 an accumulated density was not finite or out of
                            // range, bit 1 a shared-memory tile load did not complete in time
-  // TMA descriptors of the halo-padded phase field and 1/rho_ref arrays, per parity
+  // TMA descriptors of the halo-padded phase field and reference-pair arrays, per parity
   CUtensorMap tm_phi[2] = {};
-  CUtensorMap tm_rinv[2] = {};
+  CUtensorMap tm_ref[2] = {};
   bool valid = false;      // fast state holds the authoritative populations
   SparsePlan* sparse = nullptr;   // particle and wall work of sym_step (built on first use)
   size_t bytes = 0;
@@ -131,6 +134,8 @@ int sparse_enqueue(SparsePlan* p, int k, cudaStream_t st);
 int sparse_enqueue_post(SparsePlan* p, int k, cudaStream_t st);   // after the collide kernel
 int sparse_launches(const SparsePlan* p);
 void sparse_plan_free(SparsePlan* p);
+// momentum link lists of h's particles from its current masks (after an import)
+int sparse_links_build(sym_handle* h, cudaStream_t st);
 
 // batch engine, batch.cu
 int batch_launch(sym_batch* b, int nsteps);   // enqueue nsteps graph steps, no synchronisation

@@ -67,6 +67,13 @@ __device__ __forceinline__ void load_3d(void* dst, const CUtensorMap* map, int c
       : "memory");
 }
 
+// Ask the TMA unit to bring `bytes` of global memory at `src` into L2 (a hint:
+// no data arrives in shared memory and nothing waits for it).  src and bytes
+// must be multiples of 16.
+__device__ __forceinline__ void prefetch_l2(const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 // Host: encode the map of a halo-padded array (x slowest, z fastest) of
 // `nz_ext` x `nyp` x `nxp` elements with row pitch `nzp` elements, read in
 // boxes of box_z x box_y x 1.  Elements past nz_ext in a row (the pitch

@@ -125,6 +125,12 @@ module symmetry_gpu
        real(c_double), value :: tr, rad_c
        real(c_double), intent(inout) :: wcap_acc
      end function
+     ! error flags the fused kernels recorded (SYM_DEV_NONFINITE = 1, SYM_DEV_TIMEOUT = 2)
+     integer(c_int) function sym_device_status(h, flags) bind(C, name="sym_device_status")
+       import :: c_int, c_ptr, c_int32_t
+       type(c_ptr), value :: h
+       integer(c_int32_t), intent(out) :: flags
+     end function
      ! checkpoint / restart (no counterpart in the reference)
      integer(c_int) function sym_checkpoint_save(h, path) bind(C, name="sym_checkpoint_save")
        import :: c_int, c_ptr, c_char
