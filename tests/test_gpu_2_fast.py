@@ -154,6 +154,25 @@ def test_reduced_storage_early_thread(storage, bound):
     assert e["u"] <= bound, e
 
 
+def test_reduced_storage_breakup_time():
+    """Breakup time of the reduced storages within 1 % of FP64's on two
+    unstable threads of the batched mix that break within 12,000 steps
+    (26x26x244, tau 0.93; 54x54x102, tau 0.81), the three storages run side by
+    side as in the precision study; the total mass drifts by less than 1e-5.
+    Measured: FP32 0.002-0.003 %, 16-bit 0.035-0.054 %."""
+    from symmetry_b200 import study
+    ws = {w.name: w for w in study.mix_cases(6)}
+    for name in ("c4_002", "c4_012"):
+        r = study.run_case(ws[name], max_steps=14000, snap_every=4000, log=None)
+        b = r["breakup_step"]
+        assert b["fp64"] is not None and b["fp64"] > 0, (name, b)
+        for m in ("fp32", "fp16"):
+            assert b[m] is not None and abs(b[m] - b["fp64"]) <= 0.01 * b["fp64"], (name, m, b)
+        for row in r["snapshots"]:
+            for m in ("fp64", "fp32", "fp16"):
+                assert abs(row["mass_drift"][m]) <= 1e-5, (name, row)
+
+
 @pytest.mark.parametrize("storage", ["fp64", "fp16"])
 def test_get_macros_leaves_stepping_state_untouched(storage):
     """sym_get_macros on a fused state returns calmacros of the current
