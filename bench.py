@@ -5,7 +5,7 @@ Default workload ("mix"): the 96 uneven Rayleigh-Plateau domains of the
 batched configuration (Nx=Ny in [24,64], Nz in [64,384], half of them with an
 on-axis sphere; 45.0 M nodes in all), FP16 shifted storage, stepped as one
 batch: one CUDA graph per step holding one phase-field launch for all domains,
-the per-domain particle chains on parallel graph branches, and one persistent
+one launch per particle/wall subroutine for all domains, and one persistent
 collide launch over a work-tile table.  One bench step = one lattice update of
 every domain (every node counted, fluid or solid).  `value` is MLUPS of the
 graph replay, inputs resident in HBM.  Beside it, on the same box (N=1 only):
@@ -13,6 +13,7 @@ graph replay, inputs resident in HBM.  Beside it, on the same box (N=1 only):
   e2e          host buffers through the C ABI: upload both colours'
                populations and rho_N of every domain (pinned, Fortran
                layout), 100 batch steps, download five macroscopic fields
+  storages     the same 96 domains batched in FP32 and in FP64 storage
   plain_fp64   the same 96 domains in plain FP64, one domain at a time
   c3_fp64      the 256x256x512 thread in plain FP64 (the roofline run)
   serving      the Poisson job stream through the job server: FP16 batched
@@ -77,7 +78,7 @@ def b_phase(storage):
 # profiles/k_collide_fp64_thread_128x128x256.md (FP64, single-domain kernel;
 # the batched kernel runs the same tile code).  The traffic per node does not
 # depend on the number of nodes, so it scales to a full launch.
-COLLIDE_TRAFFIC_B_PER_NODE = {"fp16": 219.3, "fp64": 709.1}
+COLLIDE_TRAFFIC_B_PER_NODE = {"fp16": 238.0, "fp64": 709.1}
 
 
 def collide_traffic(storage, nodes):
@@ -353,6 +354,25 @@ def plain_fp64(ws, steps, local):
                    "updates / summed device time"}
 
 
+def batched_mix(storage, steps, local):
+    """The same 96 domains batched in another storage (graph replay, tiles
+    from the autotuner): the precision/speed trade-off beside the headline."""
+    from symmetry_b200 import configs
+    from symmetry_b200.lib import Batch, setup_workload
+    ws = configs.c4_manifest(storage=storage)
+    lattices = [setup_workload(w, device=local) for w in ws]
+    B = Batch(lattices)
+    B.autotune(trial_steps=3)
+    B.step(3)
+    ms = B.step_timed(steps)
+    B.close()
+    for L in lattices:
+        L.close()
+    nodes = sum(w.nodes for w in ws)
+    return {"value": nodes * steps / ms / 1e3, "unit": "MLUPS", "storage": storage, "steps": steps,
+            "ms_per_step": ms / steps}
+
+
 def c3_leg(steps, peak, local):
     from symmetry_b200 import configs
     from symmetry_b200.lib import setup_workload
@@ -441,7 +461,7 @@ def main():
     ap.add_argument("--workload", default="mix")
     ap.add_argument("--storage", default=None, help="storage of the timed workload (mix: fp16, others: fp64)")
     ap.add_argument("--size", default=None, help="override domain size NXxNYxNZ (thread workloads)")
-    ap.add_argument("--legs", default="kernels,e2e,plain,c3,serve,cpu",
+    ap.add_argument("--legs", default="kernels,e2e,storages,plain,c3,serve,cpu",
                     help="auxiliary measurements at N=1 (comma list; 'none' for the timed region only)")
     ap.add_argument("--domains", type=int, default=96, help="mix: the first D domains of the manifest "
                                                              "(smaller cases for profiler captures)")
@@ -563,6 +583,9 @@ def mix_main(args, torch, dist, rank, world, local, legs, peak, peak_kind):
     for L in lattices:
         L.close()
     del lattices, B
+    if "storages" in legs:
+        line["batched_same_mix_other_storage"] = {
+            st: leg("mix_" + st, batched_mix, st, 20, local) for st in ("fp32", "fp64")}
     if "plain" in legs:
         p = leg("plain", plain_fp64, configs.c4_manifest(storage="fp64"), 20, local)
         if "value" in p:

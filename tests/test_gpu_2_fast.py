@@ -130,12 +130,13 @@ def driven_channel():
     return w
 
 
-@pytest.mark.parametrize("storage,bound", [("fp32", 1e-4), ("fp16", 3e-3)])
+@pytest.mark.parametrize("storage,bound", [("fp32", 1e-4), ("fp16", 1e-3)])
 def test_reduced_storage_driven_flow(storage, bound):
     """Velocity error of the reduced storage against the FP64 oracle on a
-    developed (body-force driven) two-phase channel flow, 1000 steps.
-    Measured: FP32 3.3e-5, 16-bit 1.9e-3 (the FP16 mantissa of the stored
-    deviation q = f/(w rho0) - 1 sets the floor, 2^-11 relative)."""
+    developed (body-force driven) two-phase channel flow, 1000 steps, within
+    the 1e-3 relative L2 target.  Measured: FP32 2.5e-5, 16-bit 3.8e-4 (the
+    FP16 significand of the stored total deviation, 2^-11 relative, sets the
+    floor)."""
     o, L = fast_run(driven_channel(), 1000, storage)
     fluid = o.arr("walls_all") == 0
     e = errors(o, L, ["ux", "uy", "uz", "rho", "rho_N"], mask=fluid)
@@ -144,10 +145,11 @@ def test_reduced_storage_driven_flow(storage, bound):
     assert e["rho"] <= bound, e
 
 
-@pytest.mark.parametrize("storage,bound", [("fp32", 5e-3), ("fp16", 5e-2)])
+@pytest.mark.parametrize("storage,bound", [("fp32", 3e-3), ("fp16", 5e-3)])
 def test_reduced_storage_early_thread(storage, bound):
     """Early Rayleigh-Plateau thread (C1, 1000 steps): velocities are small
-    (~1e-5) and the error is noise-dominated; recorded, loosely bounded."""
+    (~1e-5) and the error is dominated by the seed noise.  Measured: FP32
+    1.3e-3, 16-bit 2.0e-3."""
     o, L = fast_run(configs.c1_thread(), 1000, storage)
     e = errors(o, L, ["ux", "uy", "uz", "rho", "rho_N"])
     print(f"{storage} early thread: {e}")
