@@ -53,7 +53,6 @@ struct TileEntry {
   int dom, z0, y0, xa, xb, cost, r0, r1;
 };
 
-constexpr int kTPB = BZ * BY;
 
 // blk[b] = (domain, block index within the domain) of phase block b
 template <typename S>
@@ -84,7 +83,7 @@ __global__ void __launch_bounds__(256) k_finalize_batch(const DomainDesc* __rest
 }
 
 template <typename S>
-__global__ void __launch_bounds__(kTPB, collide_ctas<S>()) k_collide_batch(const DomainDesc* __restrict__ descs,
+__global__ void __launch_bounds__(kTPB<S>, collide_ctas<S>()) k_collide_batch(const DomainDesc* __restrict__ descs,
                                                            const TileEntry* __restrict__ tiles, int ntiles,
                                                            int* __restrict__ counter) {
   using R = typename Codec<S>::R;
@@ -103,7 +102,7 @@ __global__ void __launch_bounds__(kTPB, collide_ctas<S>()) k_collide_batch(const
     {  // stage the tile's domain descriptor in shared memory
       const int* src = reinterpret_cast<const int*>(&descs[e.dom]);
       int* dst = reinterpret_cast<int*>(&s_desc);
-      for (int k = threadIdx.x; k < (int)(sizeof(DomainDesc) / sizeof(int)); k += kTPB) dst[k] = src[k];
+      for (int k = threadIdx.x; k < (int)(sizeof(DomainDesc) / sizeof(int)); k += kTPB<S>) dst[k] = src[k];
     }
     __syncthreads();
     const DomainDesc& D = s_desc;
@@ -125,7 +124,7 @@ int set_batch_smem(int device, int* per_sm, int* sms) {
   const int shm = (int)smem_bytes<S>();
   if (cudaFuncSetAttribute(k_collide_batch<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, shm) != cudaSuccess)
     return SYM_ERR_CUDA;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_collide_batch<S>, kTPB, shm);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_collide_batch<S>, kTPB<S>, shm);
   cudaDeviceGetAttribute(sms, cudaDevAttrMultiProcessorCount, device);
   *per_sm = std::max(1, *per_sm);
   *sms = std::max(1, *sms);
@@ -233,7 +232,7 @@ int enqueue_batch_step(sym_batch* b, int k, cudaEvent_t* ev) {
   if (ev) cudaEventRecord(ev[2], b->st);
   cudaMemsetAsync(b->d_counter + k, 0, sizeof(int), b->st);
   using R = typename Codec<S>::R;
-  k_collide_batch<S><<<b->grid, kTPB, smem_bytes<S>(), b->st>>>(b->d_desc[k], b->d_tiles, b->ntiles,
+  k_collide_batch<S><<<b->grid, kTPB<S>, smem_bytes<S>(), b->st>>>(b->d_desc[k], b->d_tiles, b->ntiles,
                                                                   b->d_counter + k);
   if (int e = sparse_enqueue_post(b->sparse, k, b->st)) return berr(b, e, "interpolated bounce-back");
   if (ev) cudaEventRecord(ev[3], b->st);
@@ -268,6 +267,7 @@ int build(sym_batch* b) {
     off[i + 1] = off[i] + (long long)((h->N + 255) / 256);
     const int xc = std::max(1, b->xchunk[i]);
     const DevParams& P = h->dp;
+    const int BY = tile_rows(b->storage);
     for (int xa = 0; xa < P.nx; xa += xc)
       for (int y0 = 0; y0 < P.ny; y0 += BY)
         for (int z0 = 0; z0 < P.nz; z0 += BZ) {

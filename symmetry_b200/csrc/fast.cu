@@ -12,8 +12,9 @@
 //   pin fill     sparse: fictitious phi on solid nodes next to fluid (:467-492).
 //   k_collide    derivatives (:497-594) + collision (:599-695) + Recolor
 //                (:697-732) + streaming (:735-768) + curve (:990-1034) fused:
-//                a CTA owns a 32(z) x 8(y) footprint and marches along x with a
-//                5-plane phi window and a 3-plane window of unit normals in
+//                a CTA owns a 32(z) x BY(y) footprint (BY per storage,
+//                kBY) and marches along x with a 5-plane phi window and a
+//                4-plane window of unit normals in
 //                shared memory; it reads each node's populations once, and
 //                pushes the recoloured post-collision populations to their
 //                neighbours (push streaming), reflecting links that enter a
@@ -110,17 +111,17 @@ int enqueue_step(sym_handle* h, int cur, int pc, cudaEvent_t* ev) {
   if (int e = sparse_enqueue(h->fast.sparse, cur, h->st)) return set_error(h, e, "sparse step");
   // (a3-a9) fused derivatives + collision + recolour + stream + bounce-back
   const int xc = h->fast.xchunk > 0 ? h->fast.xchunk : XCHUNK;
-  dim3 grid((P.nz + BZ - 1) / BZ, (P.ny + BY - 1) / BY, (P.nx + xc - 1) / xc);
+  dim3 grid((P.nz + BZ - 1) / BZ, (P.ny + kBY<S> - 1) / kBY<S>, (P.nx + xc - 1) / xc);
   const size_t shm = smem_bytes<S>();
   const CUtensorMap& tp = h->fast.tm_phi[pc];
   const CUtensorMap& tr = h->fast.tm_ref[pc];
   if (ev) cudaEventRecord(ev[2], h->st);
   if (solid)
-    k_collide<S, true><<<grid, TPB, shm, h->st>>>(P, pd, pin_, pnext, phic, h->walls, h->walls_all, h->pout,
+    k_collide<S, true><<<grid, kTPB<S>, shm, h->st>>>(P, pd, pin_, pnext, phic, h->walls, h->walls_all, h->pout,
                                                   h->dpart, h->ffi, rr_old(h, pc), rr_new(h, pc), accbuf<S>(h),
                                                   h->fast.status, tp, tr, xc);
   else
-    k_collide<S, false><<<grid, TPB, shm, h->st>>>(P, pd, pin_, pnext, phic, h->walls, h->walls_all, h->pout,
+    k_collide<S, false><<<grid, kTPB<S>, shm, h->st>>>(P, pd, pin_, pnext, phic, h->walls, h->walls_all, h->pout,
                                                    h->dpart, h->ffi, rr_old(h, pc), rr_new(h, pc), accbuf<S>(h),
                                                    h->fast.status, tp, tr, xc);
   if (int e = sparse_enqueue_post(h->fast.sparse, cur, h->st)) return set_error(h, e, "interpolated bounce-back");
@@ -208,6 +209,7 @@ int fast_alloc(sym_handle* h) {
   F.bytes = h->bytes - before;
   // TMA descriptors of the phase-field (and 16-bit reference-pair) tiles the
   // collide kernel reads: boxes of (BZ+4) x (BY+4) x 1 over the padded arrays
+  const int BY = tile_rows(F.storage);
   for (int k = 0; k < 2; k++) {
     const bool f64 = F.storage == SYM_STORE_FP64;
     void* phi = f64 ? (void*)F.phi[k] : (void*)F.phif[k];

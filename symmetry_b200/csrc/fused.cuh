@@ -4,6 +4,7 @@
 #pragma once
 #include <cuda_fp16.h>
 #include <cmath>
+#include <type_traits>
 #include <utility>
 #include "state.cuh"
 #include "tma.cuh"
@@ -11,7 +12,7 @@
 namespace symb200 {
 namespace fused {
 
-constexpr int BZ = 32, BY = 8, TPB = BZ * BY;
+constexpr int BZ = 32;   // tile width along z: one warp per row
 constexpr int XCHUNK = 32;   // x planes marched by one CTA
 
 // ---- halo-padded phase field -----------------------------------------------------
@@ -367,14 +368,30 @@ template <typename R>
 struct alignas(4 * sizeof(R)) NormalV {
   R x, y, z, g;
 };
+// Tile height (rows of BZ nodes) of the collide kernels per storage: 16
+// rows for the 16-bit codec, 8 for FP32 and FP64.  Measured on the batched
+// mix: 16 rows (2 CTAs of 512 threads per SM) took the 16-bit collide from
+// 4.79 to 4.28 ms against 8 rows (4 CTAs of 256) -- fewer halo normals, halo
+// bytes and barriers per node -- and changed nothing in FP32; FP64 at 16 rows
+// fits one CTA per SM and was slower (C3: 4.70 against 4.52 ms).
+template <typename S>
+constexpr int kBY = std::is_same<S, __half>::value ? 16 : 8;
+template <typename S>
+constexpr int kTPB = BZ * kBY<S>;
+// the same for a storage mode chosen at run time (SYM_STORE_*)
+inline int tile_rows(int storage) {
+  return storage == SYM_STORE_FP16 ? kBY<__half> : (storage == SYM_STORE_FP32 ? kBY<float> : kBY<double>);
+}
 // phi and reference-pair plane tiles ((BY+4) x (BZ+4), z fastest) arrive by TMA:
 // each slot starts on a 128-byte boundary
-constexpr int kPlaneTile = (BY + 4) * (BZ + 4);
+template <typename S>
+constexpr int kPlaneTile = (kBY<S> + 4) * (BZ + 4);
 template <typename S>
 struct Smem {
   using R = typename Codec<S>::R;
-  static constexpr int kPhiSlot = (kPlaneTile * (int)sizeof(R) + 127) / 128 * 128 / (int)sizeof(R);
-  static constexpr int kRefSlot = (kPlaneTile * 8 + 127) / 128 * 128 / 8;
+  static constexpr int BY = kBY<S>;
+  static constexpr int kPhiSlot = (kPlaneTile<S> * (int)sizeof(R) + 127) / 128 * 128 / (int)sizeof(R);
+  static constexpr int kRefSlot = (kPlaneTile<S> * 8 + 127) / 128 * 128 / 8;
   alignas(128) R phi[5][kPhiSlot];
   alignas(128) Ref ref[Codec<S>::kRef ? kIrrRing : 1][kRefSlot];   // reference pairs of this step (16-bit storage)
   NormalV<R> n[4][BY + 2][BZ + 2];   // [plane][y][z]: n and |grad phi|
@@ -408,7 +425,7 @@ __host__ __device__ __forceinline__ constexpr int PUSH_ORDER(int k) {
   return a[k];
 }
 
-// One tile: the 32(z) x 8(y) footprint at (z0, y0), planes xa..xb-1.  Called
+// One tile: the 32(z) x BY(y) footprint at (z0, y0), planes xa..xb-1.  Called
 // by the single-domain kernel (tile from blockIdx) and by the batched
 // persistent kernel (tile from the work-tile table).
 template <typename S, bool SOLID>
@@ -424,6 +441,7 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
                                              int z0, int y0, int xa, int xb, Smem<S>& sm, unsigned& nload,
                                              bool solid_rt = true) {
   using R = typename Codec<S>::R;
+  constexpr int BY = kBY<S>, TPB = kTPB<S>, kTile = kPlaneTile<S>;
   // solid handling: compiled in (SOLID) and wanted by this domain (solid_rt);
   // the batched kernel compiles one variant and decides per tile
   const bool SOLIDX = SOLID && solid_rt;
@@ -441,7 +459,7 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
   // mbarrier (number mod 6) with phase parity (number / 6) mod 2.
   const unsigned nl0 = nload;
   auto load_no = [&](int xp) { return nl0 + (unsigned)(xp - (xa - 2)); };
-  constexpr uint32_t kTx = kPlaneTile * (sizeof(R) + (REF ? sizeof(Ref) : 0));
+  constexpr uint32_t kTx = kTile * (sizeof(R) + (REF ? sizeof(Ref) : 0));
   auto load_phi = [&](int xp) {   // thread 0 only
     const unsigned q = load_no(xp);
     uint64_t* bar = &sm.bar[q % kIrrRing];
@@ -774,14 +792,17 @@ __device__ __forceinline__ void collide_tile(const DevParams& P, const Pad& pd, 
 }
 
 // Resident CTAs per SM the collide kernels are compiled for: the FP32-math
-// codecs fit 64 registers (4 CTAs of 256 threads; measured faster than 3 CTAs
-// at 80 registers, the issue-bound kernel gains from the extra warps), FP64
-// needs the 128 of 2 CTAs.
+// codecs fit 64 registers (32 warps per SM: 4 CTAs of 256 threads for FP32,
+// 2 of 512 for the 16-bit codec; measured faster than 3 CTAs of 256 at 80
+// registers, the latency-bound kernel gains from the extra warps), FP64 needs
+// the 128 of 2 CTAs of 256.
 template <typename S>
-constexpr int collide_ctas() { return sizeof(typename Codec<S>::R) == 4 ? 4 : 2; }
+constexpr int collide_ctas() {
+  return std::is_same<S, __half>::value ? 2 : (sizeof(typename Codec<S>::R) == 4 ? 4 : 2);
+}
 
 template <typename S, bool SOLID>
-__global__ void __launch_bounds__(TPB, collide_ctas<S>()) k_collide(DevParams P, Pad pd, const S* __restrict__ pin_,
+__global__ void __launch_bounds__(kTPB<S>, collide_ctas<S>()) k_collide(DevParams P, Pad pd, const S* __restrict__ pin_,
                                                    S* __restrict__ pout_,
                                                    const typename Codec<S>::R* __restrict__ phi,
                                                    const int32_t* __restrict__ walls,
@@ -798,7 +819,8 @@ __global__ void __launch_bounds__(TPB, collide_ctas<S>()) k_collide(DevParams P,
   unsigned nload = 0;
   const int xa = blockIdx.z * xchunk;
   collide_tile<S, SOLID>(P, pd, pin_, pout_, phi, walls, walls_all, pout, Sp, ffi, rr_old, rr_new, acc, status,
-                         &tm_phi, &tm_ref, blockIdx.x * BZ, blockIdx.y * BY, xa, min(xa + xchunk, P.nx), sm, nload);
+                         &tm_phi, &tm_ref, blockIdx.x * BZ, blockIdx.y * kBY<S>, xa, min(xa + xchunk, P.nx), sm,
+                         nload);
 }
 
 // ---- the fused state's side of the particle and wall work ---------------------------
