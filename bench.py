@@ -504,11 +504,15 @@ def main():
 
 
 def timed_max(torch, dist, ms, local):
-    if not dist:
-        return ms
-    t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    """The slowest rank's device time (symmetry_b200.dist)."""
+    from symmetry_b200.dist import max_over_ranks
+    return max_over_ranks(torch, dist, ms, device=f"cuda:{local}")
+
+
+def whole_job_mlups(torch, dist, node_updates, t_max, local):
+    """All ranks' node updates over the slowest rank's time (symmetry_b200.dist)."""
+    from symmetry_b200.dist import aggregate_mlups, sum_over_ranks
+    return aggregate_mlups(sum_over_ranks(torch, dist, node_updates, device=f"cuda:{local}"), t_max)
 
 
 def mix_main(args, torch, dist, rank, world, local, legs, peak, peak_kind):
@@ -538,7 +542,7 @@ def mix_main(args, torch, dist, rank, world, local, legs, peak, peak_kind):
         ms = B.step_timed(args.steps)
     torch.cuda.synchronize()
     t_max = timed_max(torch, dist, ms, local)
-    value = world * nodes * args.steps / (t_max / 1e3) / 1e6
+    value = whole_job_mlups(torch, dist, nodes * args.steps, t_max, local)
     line = {
         "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -627,7 +631,7 @@ def single_main(args, torch, dist, rank, world, local, legs, peak, peak_kind):
     with ClockSampler(local) as clk:
         ms = L.step_timed(args.steps, use_graph=True)[0]
     t_max = timed_max(torch, dist, ms, local)
-    value = world * nodes * args.steps / (t_max / 1e3) / 1e6
+    value = whole_job_mlups(torch, dist, nodes * args.steps, t_max, local)
     k = L.step_timed(min(args.steps, 20), use_graph=False)
     ks = min(args.steps, 20)
     col, ph = k[3] / ks, k[1] / ks
