@@ -67,11 +67,12 @@ __device__ __forceinline__ void phi_store(const DevParams& P, const Pad& pd, R* 
 //                                   does not eat the significand; the 2^12
 //                                   scale keeps deviations down to 1e-8 out
 //                                   of the FP16 subnormal range)
-//   d = r / f - chi_ref             the red fraction's deviation from the
-//                                   node's: exactly 0 in a pure phase, and the
-//                                   small colour perturbations that seed an
-//                                   instability keep FP16's 2^-11 relative
-//                                   precision instead of a fixed step
+//   d = 4096 (r - chi_ref f) / w    the red population's deviation from the
+//                                   node's colour split of f: exactly 0 in a
+//                                   pure phase, and the small colour
+//                                   perturbations that seed an instability
+//                                   keep FP16's 2^-11 relative precision
+//                                   instead of a fixed step (no quotient)
 // Encoder and decoder share the rounded rest equilibrium e = w rho_ref (one
 // product, never contracted), so the rounding of the scale factors multiplies
 // only the deviation and adds no bias to the mass.
@@ -136,7 +137,7 @@ struct Codec<__half> {
                                                  R& r) {
     const float2 q = __half22float2(reinterpret_cast<const __half2*>(p)[I * N + L]);
     f = fmaf(q.x, float(W(I) / 4096.0), __fmul_rn(float(W(I)), ref.x));
-    r = f * (ref.y + q.y);
+    r = fmaf(q.y, float(W(I) / 4096.0), ref.y * f);
   }
   template <int I>
   __device__ __forceinline__ static void load(const __half* __restrict__ p, unsigned N, unsigned L, Ref ref, R& r,
@@ -149,8 +150,8 @@ struct Codec<__half> {
   __device__ __forceinline__ static void store(__half* p, unsigned N, unsigned L, Ref ref, R r, R f) {
     constexpr float c = float(4096.0 / W(I));   // 12288, 73728 or 147456: exact
     const R q = (f - __fmul_rn(float(W(I)), ref.x)) * c;
-    // the pure phases exactly (r = f, r = 0), other fractions by the fast quotient
-    const R d = (r == f ? R(1) : (r == R(0) ? R(0) : __fdividef(r, f))) - ref.y;
+    // exactly 0 in a pure phase: r = f with chi_ref = 1, r = 0 with chi_ref = 0
+    const R d = fmaf(-ref.y, f, r) * c;
     reinterpret_cast<__half2*>(p)[I * N + L] = __floats2half2_rn(q, d);
   }
 };
