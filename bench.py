@@ -78,7 +78,7 @@ def b_phase(storage):
 # profiles/k_collide_fp64_thread_128x128x256.md (FP64, single-domain kernel;
 # the batched kernel runs the same tile code).  The traffic per node does not
 # depend on the number of nodes, so it scales to a full launch.
-COLLIDE_TRAFFIC_B_PER_NODE = {"fp16": 223.2, "fp64": 704.2}
+COLLIDE_TRAFFIC_B_PER_NODE = {"fp16": 224.7, "fp64": 704.2}
 
 
 def collide_traffic(storage, nodes):
