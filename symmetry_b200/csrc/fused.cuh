@@ -845,9 +845,10 @@ __device__ __forceinline__ void pinfill_node(const DevParams& P, const Pad& pd, 
 }
 
 // particle preparation: canonical views of the fused state at a node of a
-// particle box -- rho_N (this step's calmacros), rho_R/rho_B and fi (current
-// populations), and the previous step's gradient/normal (from the previous
-// pin-filled phi): what Lagrange_points, momentum and refilling read.
+// particle box -- rho_N (this step's calmacros), rho_R/rho_B and, at nodes
+// next to a particle, fi (current populations), and the previous step's
+// gradient/normal (from the previous pin-filled phi): what Lagrange_points,
+// momentum and refilling read.
 // rr_old (16-bit storage): the reference pairs of the populations.
 template <typename S>
 __device__ __forceinline__ void prep_node(const DevParams& P, const Pad& pd, const sym_particles* __restrict__ Sp,
@@ -866,12 +867,15 @@ __device__ __forceinline__ void prep_node(const DevParams& P, const Pad& pd, con
     gx[L] = 0.0; gy[L] = 0.0; gz[L] = 0.0; nxv[L] = 0.0; nyv[L] = 0.0; nzv[L] = 0.0;
     return;
   }
+  // fi is read only by the momentum exchange, at nodes with links into a
+  // particle (pout > 0): written there only
+  const bool links = pout[L] > 0;
   R sr = R(0), sb = R(0);
   unroll19([&](auto ic) {
     constexpr int i = decltype(ic)::value;
     R r, b;
     Codec<S>::template load<i>(pops, N, (unsigned)L, rref, r, b);
-    fi[(size_t)i * N + L] = (double)(r + b);
+    if (links) fi[(size_t)i * N + L] = (double)(r + b);
     sr = sr + r;
     sb = sb + b;
   });
