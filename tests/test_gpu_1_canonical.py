@@ -5,7 +5,7 @@ The canonical kernels are compiled without fused multiply-add, so outside the
 transcendental calls (acos/sin/cos in the wetting rotation and the Lagrange
 points, tanh in the initial state) they round exactly like the oracle.
 Tolerances: per-subroutine 1e-12 max-relative; after many steps the field
-relative L2 error <= 1e-10, masks bit-exact, particle
+relative L2 error <= 1e-10 (the FP64 parity target), masks bit-exact, particle
 trajectories <= 1e-9.
 """
 import numpy as np
