@@ -261,7 +261,7 @@ int sym_batch_get_xchunk(sym_batch* b, int domain, int* xchunk);
  * fit; default the most): grid = per_sm x SM count. */
 int sym_batch_set_ctas_per_sm(sym_batch* b, int per_sm);
 /* Picks the tile x extent per size class (nx <= 32, <= 48, larger) from
- * {8,16,32,64}, then the resident CTAs per SM, by timing; the trial steps
+ * {8,12,16,24,32,64}, then the resident CTAs per SM, by timing; the trial steps
  * advance every domain (*steps_taken). */
 int sym_batch_autotune(sym_batch* b, int trial_steps, int* steps_taken);
 int sym_batch_info(sym_batch* b, int64_t* nodes, int* ntiles, int* grid);

@@ -472,13 +472,13 @@ int sym_batch_step_timed(sym_batch* b, int nsteps, double* ms) {
 }
 
 // Choose the tile x extent per size class (domains grouped by nx: <=32, <=48,
-// larger) from {8, 16, 32, 64}, then the persistent collide grid (resident
-// CTAs per SM, from the most that fit down to 1), each by timing trial_steps
+// larger) from {8, 12, 16, 24, 32, 64}, then the persistent collide grid
+// (resident CTAs per SM, from the most that fit down to 1), each by timing trial_steps
 // graph steps per candidate.  The trial steps advance every domain;
 // *steps_taken reports how many.
 int sym_batch_autotune(sym_batch* b, int trial_steps, int* steps_taken) {
   if (!b || trial_steps <= 0) return SYM_ERR_PARAM;
-  const int cands[4] = {8, 16, 32, 64};
+  const int cands[6] = {8, 12, 16, 24, 32, 64};
   auto cls = [](int nx) { return nx <= 32 ? 0 : (nx <= 48 ? 1 : 2); };
   int taken = 0;
   for (int c = 0; c < 3; c++) {

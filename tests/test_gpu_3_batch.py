@@ -67,7 +67,7 @@ def test_batch_autotune_and_info():
     taken = B.autotune(trial_steps=2)
     assert taken > 0
     for i in range(len(members)):
-        assert B.xchunk(i) in (8, 16, 32, 64)
+        assert B.xchunk(i) in (8, 12, 16, 24, 32, 64)
     info = B.info()
     assert info["nodes"] == sum(w.nodes for w in ws) and info["tiles"] > 0 and info["grid"] >= 148
     # stepping after tuning still matches a domain stepped alone with the same tiles
