@@ -114,8 +114,11 @@ __device__ __forceinline__ int lag_idx(const DevParams& P, long long c, int n, i
   }
   long long i = c - P.origin;
   const bool periodic = !(k == 0 && P.wall_x);
-  if (periodic) i = ((i % n) + n) % n;
-  else i = i < 0 ? 0 : (i > n - 1 ? n - 1 : i);
+  if (periodic) {
+    if (i < 0 || i >= n) i = ((i % n) + n) % n;
+  } else {
+    i = i < 0 ? 0 : (i > n - 1 ? n - 1 : i);
+  }
   return (int)i;
 }
 
@@ -163,13 +166,20 @@ __device__ __forceinline__ void lagrange_point(const DevParams& P, const sym_par
   double v = 0.0;
   int fl = 0;
   long long x0 = 0, y0 = 0, z0 = 0;
+  // array indices of the corners' coordinates: every corner takes c or c + 1
+  // along each axis, so six lookups serve all eight corners
+  int ix0 = 0, ix1 = 0, iy0 = 0, iy1 = 0, iz0 = 0, iz1 = 0;
   if (in_domain) {
     if (P.ref) { x0 = (long long)lx; y0 = (long long)ly; z0 = (long long)lz; }
     else { x0 = (long long)floor(lx); y0 = (long long)floor(ly); z0 = (long long)floor(lz); }
+    ix0 = lag_idx(P, x0, P.nx, 0); ix1 = lag_idx(P, x0 + 1, P.nx, 0);
+    iy0 = lag_idx(P, y0, P.ny, 1); iy1 = lag_idx(P, y0 + 1, P.ny, 1);
+    iz0 = lag_idx(P, z0, P.nz, 2); iz1 = lag_idx(P, z0 + 1, P.nz, 2);
     double wsum = 0.0, acc = 0.0;
+#pragma unroll
     for (int i = 0; i < 8; i++) {
       const long long xf = x0 + EX[i], yf = y0 + EY[i], zf = z0 + EZ[i];
-      const long long F = lin(P, lag_idx(P, xf, P.nx, 0), lag_idx(P, yf, P.ny, 1), lag_idx(P, zf, P.nz, 2));
+      const long long F = lin(P, EX[i] ? ix1 : ix0, EY[i] ? iy1 : iy0, EZ[i] ? iz1 : iz0);
       if (walls[F] <= 0) {
         const double star = rhoN[F] + gx[F] * (lx - (double)xf) + gy[F] * (ly - (double)yf) + gz[F] * (lz - (double)zf);
         const double dis = (double)(xf - lx) * (double)(xf - lx) + ((double)yf - ly) * ((double)yf - ly) +
@@ -191,21 +201,22 @@ __device__ __forceinline__ void lagrange_point(const DevParams& P, const sym_par
     double nw[3] = {lx - cx, ly - cy, lz - cz};
     unitization(nw);
     double mn = 100.0;
-    long long xx = x0, yy = y0, zz = z0;
+    long long G = lin(P, ix0, iy0, iz0);   // corner 0 unless a nearer one qualifies
+#pragma unroll 1
     for (int i = 0; i < 8; i++) {
-      const long long xf = x0 + EX[i], yf = y0 + EY[i], zf = z0 + EZ[i];
+      const int ex = ((i + 1) >> 1) & 1, ey = (i >> 1) & 1, ez = (i >> 2) & 1;   // EX[i], EY[i], EZ[i]
+      const long long xf = x0 + ex, yf = y0 + ey, zf = z0 + ez;
       const bool inside = P.ref ? (xf <= P.nx && yf >= 1 && yf <= P.ny && zf <= P.nz) : true;
       if (!inside) continue;
-      const long long F = lin(P, lag_idx(P, xf, P.nx, 0), lag_idx(P, yf, P.ny, 1), lag_idx(P, zf, P.nz, 2));
+      const long long F = lin(P, ex ? ix1 : ix0, ey ? iy1 : iy0, ez ? iz1 : iz0);
       if (walls[F] <= 0) {
         if (fabs(nxv[F] * nxv[F] + nyv[F] * nyv[F] + nzv[F] * nzv[F]) > 0.0) {
           const double dis = ((double)xf - lx) * ((double)xf - lx) + ((double)yf - ly) * ((double)yf - ly) +
                              ((double)zf - lz) * ((double)zf - lz);
-          if (sqrt(dis) < mn) { mn = sqrt(dis); xx = xf; yy = yf; zz = zf; }
+          if (sqrt(dis) < mn) { mn = sqrt(dis); G = F; }
         }
       }
     }
-    const long long G = lin(P, lag_idx(P, xx, P.nx, 0), lag_idx(P, yy, P.ny, 1), lag_idx(P, zz, P.nz, 2));
     double nt[3] = {nxv[G], nyv[G], nzv[G]};
     unitization(nt);
     double r[3];
