@@ -72,7 +72,7 @@ __global__ void k_capillary(DevParams P, const sym_particles* __restrict__ S, co
                             const double* __restrict__ La_ny, const double* __restrict__ La_nz,
                             const int32_t* __restrict__ La_flag, const double* __restrict__ ds, int do_tension,
                             double* part) {
-  __shared__ double sh[256];
+  __shared__ double sh[kCapShared];
   capillary_partial(P, S, Lax, Lay, Laz, La_rhoN, La_nx, La_ny, La_nz, La_flag, ds, do_tension, part,
                     blockIdx.y + 1, blockIdx.x, sh);
 }

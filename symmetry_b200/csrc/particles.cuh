@@ -240,12 +240,32 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
   return r;
 }
 
+// K block sums at once, each added in block_sum's pairwise order (the same
+// result bit for bit) with one barrier per level for all K; sh holds K * NT
+// doubles.  The sums are left in sh[c * NT].
+template <int NT, int K>
+__device__ __forceinline__ void block_sums(const double (&v)[K], double* sh) {
+#pragma unroll
+  for (int c = 0; c < K; c++) sh[c * NT + threadIdx.x] = v[c];
+  __syncthreads();
+#pragma unroll
+  for (int s = NT / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) {
+#pragma unroll
+      for (int c = 0; c < K; c++) sh[c * NT + threadIdx.x] = sh[c * NT + threadIdx.x] + sh[c * NT + threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+}
+
 // Shb (immersed area) and capillary_force2 (Source1.f90:1980-2028).  The
 // 16,380 Lagrange points of a particle are split over kCapBlocks blocks that
 // write fixed-order partial sums (part[(pp-1)*kCapBlocks + block][7]); the
 // final pass adds them in block order (deterministic).  Block-level: every
-// thread of the 256-thread block calls it.
+// thread of the 256-thread block calls it, with kCapShared doubles of shared
+// memory in sh.
 constexpr int kCapBlocks = 32;
+constexpr int kCapShared = 7 * 256;
 __device__ __forceinline__ void capillary_partial(const DevParams& P, const sym_particles* __restrict__ S,
                                                   const double* __restrict__ Lax, const double* __restrict__ Lay,
                                                   const double* __restrict__ Laz, const double* __restrict__ La_rhoN,
@@ -278,10 +298,8 @@ __device__ __forceinline__ void capillary_partial(const DevParams& P, const sym_
     veccross(xr, temp, tt);
     for (int c = 0; c < 3; c++) { acc[c] += temp[c]; acc[3 + c] += tt[c]; }
   }
-  for (int c = 0; c < 7; c++) {
-    const double v = block_sum<256>(acc[c], sh);
-    if (threadIdx.x == 0) part[((size_t)(pp - 1) * kCapBlocks + blk) * 7 + c] = v;
-  }
+  block_sums<256, 7>(acc, sh);
+  if (threadIdx.x < 7) part[((size_t)(pp - 1) * kCapBlocks + blk) * 7 + threadIdx.x] = sh[threadIdx.x * 256];
 }
 // component c (0..6) of particle pp's capillary sums, in block order
 __device__ __forceinline__ void capillary_final_body(const DevParams& P, sym_particles* S,

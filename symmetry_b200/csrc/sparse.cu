@@ -80,7 +80,7 @@ struct Blk {
 
 // ---- kernels -------------------------------------------------------------------
 template <typename S>
-__global__ void __launch_bounds__(kT) k_sp_prep(const SpDom* __restrict__ doms, const Blk* __restrict__ map) {
+__global__ void __launch_bounds__(kT, 4) k_sp_prep(const SpDom* __restrict__ doms, const Blk* __restrict__ map) {
   using R = typename Codec<S>::R;
   const Blk e = map[blockIdx.x];
   const SpDom& D = doms[e.d];
@@ -90,7 +90,7 @@ __global__ void __launch_bounds__(kT) k_sp_prep(const SpDom* __restrict__ doms, 
                D.rhoR, D.rhoB, D.fi, D.gx, D.gy, D.gz, D.nx, D.ny, D.nz, D.rr_old, x, y, z);
 }
 
-__global__ void __launch_bounds__(kT) k_sp_lagrange(const SpDom* __restrict__ doms, const Blk* __restrict__ map) {
+__global__ void __launch_bounds__(kT, 4) k_sp_lagrange(const SpDom* __restrict__ doms, const Blk* __restrict__ map) {
   const Blk e = map[blockIdx.x];
   const SpDom& D = doms[e.d];
   part::lagrange_point(D.P, D.S, D.walls, D.rhoN, D.gx, D.gy, D.gz, D.nx, D.ny, D.nz, D.lax, D.lay, D.laz, D.larhon,
@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(kT) k_sp_lagrange_table(const SpDom* __restric
 }
 
 __global__ void __launch_bounds__(kT) k_sp_capillary(const SpDom* __restrict__ doms, const Blk* __restrict__ map) {
-  __shared__ double sh[kT];
+  __shared__ double sh[part::kCapShared];
   const Blk e = map[blockIdx.x];
   const SpDom& D = doms[e.d];
   part::capillary_partial(D.P, D.S, D.lax, D.lay, D.laz, D.larhon, D.lanx, D.lany, D.lanz, D.laflag, D.lads, 1,
