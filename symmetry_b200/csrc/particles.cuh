@@ -373,6 +373,12 @@ __device__ __forceinline__ void momentum_final_body(const DevParams& P, sym_part
 // ---- momentum over link lists (fused and batched paths) ------------------------
 // margin of the momentum box and of set_walls' pin/pout box (the same box)
 constexpr double kLinkMargin = 3.0;
+// margin of the box on which a fused step writes the canonical views (prep):
+// every later reader of them in the step stays within R + 2 of the centre the
+// box is placed on -- Lagrange corners (R + sqrt 3), link nodes (R + 1),
+// refilled nodes and the fluid neighbours they average (R + 2 of the same,
+// pre-move centre) -- and a particle moves far less than a node per step
+constexpr double kPrepMargin = 3.0;
 // The links of particle pp -- (fluid node, velocity i) with the node's
 // neighbour x - c_i inside the particle -- are kept per block of pp's
 // momentum box as a compact list: block b's entries are (node, 18-bit mask of

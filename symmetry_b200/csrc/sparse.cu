@@ -17,7 +17,7 @@
 //   set_walls       masks (:326-395): reset on the previous box, flat wall
 //                   planes, sphere marks, pin/pout and the link lists of the
 //                   next step's momentum
-//   refilling       uncovered nodes (:1351-1418), then into the fused state
+//   refilling       uncovered nodes (:1351-1418) and into the fused state
 //   pin fill        fictitious phi on solid nodes next to fluid
 // and, after the collide kernel, with the interpolated bounce-back:
 //   curve2          links into a particle re-set with the link fraction
@@ -247,15 +247,10 @@ __global__ void __launch_bounds__(kT) k_links_build(DevParams P, part::Box b, in
   part::link_compact(has, L, mask, links + seg * kT, nlinks + seg, sh);
 }
 
-__global__ void __launch_bounds__(kT) k_sp_refill(const SpDom* __restrict__ doms, const Blk* __restrict__ map) {
-  const Blk e = map[blockIdx.x];
-  const SpDom& D = doms[e.d];
-  int x, y, z;
-  if (!part::box_node(D.P, D.bref, D.S->center_old, e.pp, (long long)e.b * kT + threadIdx.x, x, y, z)) return;
-  part::refill_node(D.P, e.pp, D.S, D.pout, D.walls_old, D.rho, D.rhoN, D.rhoR, D.rhoB, D.ux, D.uy, D.uz, D.ri,
-                    D.bi, D.fi, x, y, z);
-}
-
+// refilling (uncovered nodes, :1351-1418) and the import of each refilled
+// node into the fused state, by the same thread: a refilled node's import
+// reads only what its own refill wrote, and no refill reads a refilled node
+// (it averages fluid neighbours only), so nodes need no ordering
 template <typename S>
 __global__ void __launch_bounds__(kT) k_sp_refill_import(const SpDom* __restrict__ doms,
                                                          const Blk* __restrict__ map) {
@@ -264,6 +259,8 @@ __global__ void __launch_bounds__(kT) k_sp_refill_import(const SpDom* __restrict
   const SpDom& D = doms[e.d];
   int x, y, z;
   if (!part::box_node(D.P, D.bref, D.S->center_old, e.pp, (long long)e.b * kT + threadIdx.x, x, y, z)) return;
+  part::refill_node(D.P, e.pp, D.S, D.pout, D.walls_old, D.rho, D.rhoN, D.rhoR, D.rhoB, D.ux, D.uy, D.uz, D.ri,
+                    D.bi, D.fi, x, y, z);
   refill_import_node<S>(D.P, D.pd, e.pp, (S*)D.pops, (R*)D.phic, D.pout, D.walls_old, D.ri, D.bi, D.rhoN,
                         D.rr_old, x, y, z);
 }
@@ -415,7 +412,7 @@ SpDom make_dom(sym_handle* h, int cur, int pc) {
   d.links = h->fast.links;
   d.nlinks = h->fast.nlinks;
   d.link_blocks = h->fast.link_blocks;
-  d.bprep = part::sphere_box(h->dp, 6.0);
+  d.bprep = part::sphere_box(h->dp, part::kPrepMargin);
   d.bmom = part::sphere_box(h->dp, part::kLinkMargin);
   d.bmark = part::sphere_box(h->dp, 1.0);
   d.bpin = part::sphere_box(h->dp, part::kLinkMargin);
@@ -569,7 +566,6 @@ SparsePlan* sparse_plan_build(const std::vector<sym_handle*>& doms, const std::v
   for (auto& t : p->fix) l += t.n ? 1 : 0;
   for (auto* v : {&p->mark, &p->pin, &p->refill})
     for (auto& t : *v) l += t.n ? 1 : 0;
-  for (auto& t : p->refill) l += t.n ? 1 : 0;   // refill and its import share a table
   l += p->nmove ? 1 : 0;
   p->launches = l;
   return p;
@@ -596,7 +592,6 @@ void enqueue_plan(SparsePlan* p, int k, cudaStream_t st) {
   for (auto& t : p->mark) go(k_sp_mark, t);
   go(k_sp_pin_plane, f[SparsePlan::PINPLANE]);
   for (auto& t : p->pin) go(k_sp_pin_box, t);
-  for (auto& t : p->refill) go(k_sp_refill, t);
   for (auto& t : p->refill) go(k_sp_refill_import<S>, t);
   go(k_sp_pinfill_plane<R>, f[SparsePlan::PFPLANE]);
   go(k_sp_pinfill_box<R>, f[SparsePlan::PFBOX]);
