@@ -2,8 +2,10 @@
 
 Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline / reference
 arm may import this module, and only as the checker or the timed CPU
-baseline.  The oracle restates Source1.f90 (see sym_oracle.cpp); its parity
-with the Fortran binary is unpinned because no Fortran compiler exists here.
+baseline.  The oracle restates Source1.f90 (see sym_oracle.cpp); with no
+Fortran compiler here, it is pinned bit for bit against the reference's own
+source run through a mechanical translation (oracle/f90py.py,
+tests/test_reference_pin.py).
 """
 from __future__ import annotations
 

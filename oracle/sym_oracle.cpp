@@ -7,16 +7,21 @@
  * the library links or calls this file.
  *
  * Parity status: the reference is Fortran and no Fortran compiler exists on
- * this image, so this restatement is pinned by (1) golden constants parsed
- * from Source1.f90 (tests/golden/), (2) an independent numpy restatement on
- * small grids and (3) invariants derived from the code.  It is not pinned
- * against an executed Fortran binary ("parity unpinned" against the binary).
+ * this image, so it cannot be built.  This restatement is pinned against the
+ * reference's own source executed instead: oracle/f90py.py translates
+ * Source1.f90 statement by statement (main up to its time loop and every
+ * subroutine, as written) into oracle/_ref/, and tests/test_reference_pin.py
+ * runs main's set-up and the whole time-loop body beside this file, routine
+ * by routine, with every array and particle variable equal bit for bit.
+ * Also: golden constants parsed from Source1.f90 (tests/golden/), an
+ * independent numpy restatement, and invariants derived from the code.
  *
  * Each routine follows the reference subroutine cited above it: same loop
  * ranges, same order of floating-point operations (left-to-right evaluation of
  * Fortran expressions, sequential SUM/MATMUL/DOT_PRODUCT), compiled with
  * -ffp-contract=off so no multiply-add is fused.  Loops whose result does not
- * depend on order run under OpenMP; reductions are done in a fixed order.
+ * depend on order run under OpenMP; reductions are done in a fixed order
+ * (the reference's loop order where it leaves the order to OpenMP).
  *
  * Arrays use the Fortran layout: scalars (z,y,x) with z fastest, populations
  * (0:18,z,y,x); x,y,z below are 1-based like the reference.
@@ -725,13 +730,15 @@ void curve2(Orc& o) {
 }
 
 // momentum (Source1.f90:1178-1261): Galilean-invariant momentum exchange.
-// Per-x-plane partial sums combined in x order (deterministic for any thread count).
+// The reference adds the force and torque under an OpenMP REDUCTION, whose
+// order of additions is left to the threads; here they are added in its loop
+// order (x, y, z, i) into one accumulator per particle -- the order of a
+// one-thread run, which the tests reproduce bit for bit.
 void momentum(Orc& o) {
   const int P = o.par;
-  std::vector<double> part((size_t)o.nx * P * 6, 0.0);
-#pragma omp parallel for schedule(static)
+  std::vector<double> sums((size_t)P * 6, 0.0);
   for (int x = o.lo_x; x <= o.hi_x; x++) {
-    double* acc = &part[(size_t)(x - 1) * P * 6];
+    double* acc = sums.data();
     for (int y = o.lo_y; y <= o.hi_y; y++)
       for (int z = o.lo_z; z <= o.hi_z; z++) {
         const size_t L = o.lin(x, y, z);
@@ -762,9 +769,7 @@ void momentum(Orc& o) {
       }
   }
   for (int pp = 1; pp <= P; pp++) {
-    double t[6] = {0, 0, 0, 0, 0, 0};
-    for (int x = 1; x <= o.nx; x++)
-      for (int k = 0; k < 6; k++) t[k] = t[k] + part[((size_t)(x - 1) * P + (pp - 1)) * 6 + k];
+    const double* t = &sums[(size_t)(pp - 1) * 6];
     for (int k = 0; k < 3; k++) { o.C(o.s.fp, pp, k) = t[k]; o.C(o.s.tp, pp, k) = t[3 + k]; }
   }
 }
