@@ -19,7 +19,8 @@ chosen as gfortran -O3 without -ffast-math on x86-64 does it:
     SUM and DOT_PRODUCT accumulate in array-element order;
   * sqrt, acos, sin, cos, ... are the C library's (Python's math module).
 Integer division truncates toward zero and MOD takes the sign of its first
-argument, as in Fortran.  I/O statements (OPEN, WRITE, CLOSE) are dropped.
+argument, as in Fortran.  OPEN and CLOSE are dropped; a WRITE appends its
+unit and the values of its output items to the module's OUT_LOG.
 The module's compile-time constants (grid extents, particle count) become
 attributes of the generated module's `C` namespace, so a test can size the
 domain; every other line keeps the source's arithmetic.
@@ -837,6 +838,27 @@ class Emitter:
                 self._init_var(self.ind, var, ctx, py)
                 self.stack[-1][1] += 1
             return
+        m = re.match(r"^write\s*\(", s)
+        if m:
+            e = _paren_end(s, s.index("("))
+            ctl = split_top(s[s.index("(") + 1:e - 1])
+            items = split_top(s[e:].strip()) if s[e:].strip() else []
+            try:
+                codes = [parse_expr(it, ctx).code for it in items]
+                unit = repr(ctl[0].strip()) if ctl else "'*'"
+                # items that index outside their arrays (undefined in Fortran)
+                # record None instead of values
+                self.emit("try:")
+                self.open_block("try")
+                self.emit(f"_out({unit}, [{', '.join(codes)}])")
+                self.close_block()
+                self.emit("except IndexError:")
+                self.open_block("except")
+                self.emit(f"_out({unit}, None)")
+                self.close_block()
+            except SyntaxError:
+                self.emit("pass  # write")
+            return
         if _IO.match(s) or s.startswith("deallocate"):
             self.emit("pass  # " + s.split("(")[0])
             return
@@ -1065,6 +1087,14 @@ def _matmul(A, v):
     ascending columns."""
     A = np.asarray(A, dtype=np.float64)
     return np.add.accumulate(A * np.asarray(v, dtype=np.float64)[None, :], axis=1)[:, -1]
+
+
+OUT_LOG = []
+
+
+def _out(unit, values):
+    """A WRITE statement: its unit and the values of its output items."""
+    OUT_LOG.append((unit, values))
 
 
 def _data(a, vals):

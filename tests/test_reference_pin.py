@@ -17,13 +17,14 @@ leaves one order of additions to its threads -- momentum's OpenMP REDUCTION
 of the force and torque (Source1.f90:1192-1193) -- and the translation runs
 it as one thread does, in loop order; the oracle adds in that order too.
 
-The domains are small (the translation runs as Python), with two particles
-placed inside them across the thread's interface: the reference's own
-12-particle layout only fits its 152^3 grid (at these sizes its particles
-overlap and reach past x = 1, where the Fortran reads outside its arrays).
-The tests are skipped where the reference source is absent.
+The domains are small (the translation runs as Python): the reference's own
+12-particle layout on the 48 x 88 x 48 grid of the GPU parity tests (the
+smallest it fits: below that its particles overlap and reach past x = 1,
+where the Fortran reads outside its arrays), and 36 x 42 x 36 with two
+particles placed across the thread's interface and launched so that nodes
+are refilled, with either bounce-back.  About four minutes in all.  The
+tests are skipped where the reference source is absent.
 """
-import os
 import warnings
 
 import numpy as np
@@ -68,14 +69,17 @@ def _diff(a, b) -> float:
 class Pair:
     """The translated reference (main's variables V) and the oracle side by side."""
 
-    def __init__(self, nx, ny, nz, centers, velocity=None):
+    def __init__(self, nx, ny, nz, centers, velocity=None, bounce=False):
         self.R = R = f90py.load_reference()          # a fresh module: its own constants
         self.par = par = len(centers)
+        self.bounce = bounce                        # curve2 in place of curve
         R.C.xl, R.C.yl, R.C.zl, R.C.par = nx, ny, nz, par
         with warnings.catch_warnings():
             warnings.simplefilter("ignore")
             self.V = R.main_setup()
-        self.o = setup_reference(reference_params(nx, ny, nz, par))
+        prm = reference_params(nx, ny, nz, par)
+        prm.bounce = 1 if bounce else 0
+        self.o = setup_reference(prm)
         self.setup_diffs = self.compare()
         # the same particles on both sides, then their masks and the derivatives
         V, s = self.V, self.o.particles
@@ -123,7 +127,9 @@ class Pair:
         for step in range(steps):
             n_stream = 0
             for k, (name, acts, line) in enumerate(self.R.MAIN_LOOP_CALLS):
-                self.ref_call(name, acts)
+                # curve2 takes curve's arguments (Source1.f90:1036); the
+                # oracle's curve runs curve2 when the bounce switch is on
+                self.ref_call("curve2" if name == "curve" and self.bounce else name, acts)
                 if name == "streaming":
                     self.o.streaming(n_stream)
                     n_stream += 1
@@ -147,12 +153,6 @@ CENTERS = [[14.3, 12.2, 14.3], [15.0, 29.8, 13.6]]
 
 
 @pytest.fixture(scope="module")
-def resting():
-    p = Pair(*DOMAIN, CENTERS)
-    return p, p.run_steps(2)
-
-
-@pytest.fixture(scope="module")
 def moving():
     # the same pair launched across the interface fast enough that nodes it
     # leaves are refilled within the steps
@@ -160,7 +160,6 @@ def moving():
     return p, p.run_steps(2)
 
 
-@pytest.mark.skipif(not os.environ.get("SYM_PIN_FULL"), reason="about 10 minutes; set SYM_PIN_FULL=1")
 def test_reference_layout_one_step():
     """The reference's own 12-particle layout (initia_center, unplaced) on the
     48 x 88 x 48 grid of the GPU parity tests: main's set-up and one step of
@@ -168,14 +167,14 @@ def test_reference_layout_one_step():
     R = f90py.load_reference()
     R.C.xl, R.C.yl, R.C.zl, R.C.par = 48, 88, 48, 12
     p = Pair.__new__(Pair)
-    p.R, p.par = R, 12
+    p.R, p.par, p.bounce = R, 12, False
     with warnings.catch_warnings():
         warnings.simplefilter("ignore")
         p.V = R.main_setup()
     p.o = setup_reference(reference_params(48, 88, 48, 12))
     _check(p.compare(), "main set-up")
-    for k in range(1, 13):
-        assert int((p.V["walls"] == k).sum()) > 1500
+    for k in range(1, 13):      # whole spheres, or halves cut by the mirror planes
+        assert int((p.V["walls"] == k).sum()) > 500
     for where, diffs in p.run_steps(1):
         _check(diffs, where)
 
@@ -199,13 +198,21 @@ def test_reference_constants_reproduced():
     assert o.la_num == C.la_num
 
 
-def test_main_setup_matches_oracle(resting):
-    p, _ = resting
+def test_main_setup_matches_oracle(moving):
+    p, _ = moving
     _check(p.setup_diffs, "main set-up")
     _check(p.placed_diffs, "placed particles")
 
 
-@pytest.mark.parametrize("case", ["resting", "moving"])
+@pytest.fixture(scope="module")
+def bouncing():
+    # the moving pair with the interpolated bounce-back (curve2), which the
+    # reference keeps beside curve without calling it
+    p = Pair(*DOMAIN, CENTERS, velocity=[[0.3, 0.25, -0.2], [-0.25, -0.3, 0.25]], bounce=True)
+    return p, p.run_steps(1)
+
+
+@pytest.mark.parametrize("case", ["moving", "bouncing"])
 def test_time_loop_routines_match_oracle(case, request):
     p, log = request.getfixturevalue(case)
     assert [c[0] for c in p.R.MAIN_LOOP_CALLS] == [
@@ -215,7 +222,7 @@ def test_time_loop_routines_match_oracle(case, request):
         _check(diffs, where)
 
 
-@pytest.mark.parametrize("case", ["resting", "moving"])
+@pytest.mark.parametrize("case", ["moving", "bouncing"])
 def test_particles_stay_in_the_domain(case, request):
     """The comparison is not vacuous: both particles are still solid in the
     domain after the steps, next to an interface, and moved."""
@@ -234,3 +241,22 @@ def test_moving_case_refills_nodes(moving):
     last set_walls left fluid nodes that were solid before it."""
     p, _ = moving
     assert int(((p.V["walls_old"] >= 1) & (p.V["walls_all"] == 0)).sum()) > 0
+
+
+def test_output3_stop_rule_matches_oracle(moving):
+    """output3's neck reading (Source1.f90:1673-1717), from the values its
+    WRITE statement puts out: hmin / Rad_c and y0 / lamda_d."""
+    p, _ = moving
+    V, R = p.V, p.R
+    p.ref_call("calmacros")
+    p.o.call("calmacros")
+    R.OUT_LOG.clear()
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        # main: call output3(rho_N,t,tr,walls_all,pout,lamda_d)
+        R.output3(V["rho_n"], 0, V["tr"], V["walls_all"], V["pout"], V["lamda_d"])
+    unit, (t, tt, h_over_rc, y_over_lamda) = R.OUT_LOG[-1]
+    hmin, y0 = p.o.output3()
+    assert h_over_rc == hmin / R.C.rad_c
+    assert y_over_lamda == y0 / V["lamda_d"]
+    assert 0.0 < hmin < DOMAIN[2]
