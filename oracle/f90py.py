@@ -171,6 +171,7 @@ class Unit:
     body: List[Tuple[int, str]] = field(default_factory=list)
     uses: List[str] = field(default_factory=list)
     vars: Dict[str, Var] = field(default_factory=dict)
+    data: List[Tuple[int, str]] = field(default_factory=list)   # DATA statements, wherever they stand
 
 
 _TYPE_RE = re.compile(r"^(integer|double\s+precision|real\s*\*\s*8|real\s*\(\s*8\s*\)|real\s*\(\s*kind\s*=\s*8\s*\)|"
@@ -226,15 +227,13 @@ def parse_units(text: str) -> Dict[str, Unit]:
                 not re.match(r"^(integer|real|logical)\s*=", s):
             cur.decls.append((n, s))
             continue
-        if in_decls and s.startswith("data "):
-            cur.decls.append((n, s))
+        if re.match(r"^data\s", s):
+            cur.data.append((n, s))
             continue
         in_decls = False
         cur.body.append((n, s))
     for u in units.values():
         for n, s in u.decls:
-            if s.startswith("data "):
-                continue
             _parse_decl(u, s)
     return units
 
@@ -705,7 +704,7 @@ class Emitter:
             self._init_var(1, v, ctx, pyname(name))
         self.stack: List[list] = [["sub", 0]]
         self.ctx, self.unit, self.ind = ctx, u, 1
-        for n, s in u.body:
+        for n, s in u.data + u.body:          # DATA initialises before the first statement
             try:
                 self.stmt(n, s)
             except SyntaxError as e:
@@ -942,7 +941,7 @@ class Emitter:
         self.stack = [["sub", 0]]
         self.ctx, self.unit, self.ind = ctx, u, 1
         self.outs.setdefault(u.name, [])
-        for n, s in u.body:
+        for n, s in u.data + u.body:          # DATA initialises before the first statement
             if re.match(r"^do\s+t\s*=", s):
                 break
             try:
