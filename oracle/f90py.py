@@ -494,7 +494,7 @@ class Parser:
             return Ex("True" if v == ".true." else "False", "l")
         if k == "str":
             self.take()
-            return Ex(v, "c")
+            return Ex(repr(v[1:-1]), "c")          # the literal's characters, as a Python string
         if v == "(/":
             self.take()
             items = []
