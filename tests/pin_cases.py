@@ -43,6 +43,9 @@ LOOP_CALLS = ["calmacros", "lagrange_points", "capillary_force2", "momentum", "r
 # other's, launched fast enough that nodes they leave are refilled
 PLACED = [[14.3, 12.2, 14.3], [15.0, 29.8, 13.6]]
 LAUNCH = [[0.3, 0.25, -0.2], [-0.25, -0.3, 0.25]]
+# the reference's own grid and layout as written (xl = yl = zl = 152, par = 12):
+# too slow for the default suite as Python, run on request
+FULL = dict(domain=(152, 152, 152), par=12, centers=None, velocity=None, bounce=False, steps=1)
 CASES = {
     # the reference's own 12 particles (initia_center) on the smallest grid
     # they fit: below it they overlap and reach past x = 1
@@ -74,8 +77,8 @@ def hexes(a) -> str:
 class OracleCase:
     """One case on the oracle alone."""
 
-    def __init__(self, name: str):
-        c = CASES[name]
+    def __init__(self, name):
+        c = CASES[name] if isinstance(name, str) else name
         self.c = c
         nx, ny, nz = c["domain"]
         prm = reference_params(nx, ny, nz, c["par"])
@@ -116,8 +119,8 @@ class OracleCase:
 class ReferenceCase:
     """One case on the translated reference (main's variables by name)."""
 
-    def __init__(self, R, name: str):
-        c = CASES[name]
+    def __init__(self, R, name):
+        c = CASES[name] if isinstance(name, str) else name
         self.c, self.R, self.par = c, R, c["par"]
         R.C.xl, R.C.yl, R.C.zl = c["domain"]
         R.C.par = c["par"]

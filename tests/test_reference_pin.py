@@ -33,7 +33,7 @@ import pytest
 from oracle import f90py
 from oracle.oracle import setup_reference
 from symmetry_b200.params import reference_params
-from tests.pin_cases import (CASES, FIELDS, LOOP_CALLS, PARTICLE_MATS, PARTICLE_VECS, OracleCase,
+from tests.pin_cases import (CASES, FIELDS, FULL, LOOP_CALLS, PARTICLE_MATS, PARTICLE_VECS, OracleCase,
                              ReferenceCase)
 
 REF = f90py.load_reference()
@@ -127,6 +127,15 @@ def test_particles_stay_in_the_domain(run):
         # nodes the pair left were refilled: the last set_walls made fluid
         # nodes that were solid before it
         assert int(((V["walls_old"] >= 1) & (V["walls_all"] == 0)).sum()) > 0
+
+
+@pytest.mark.skipif(not os.environ.get("SYM_PIN_152"), reason="about an hour as Python; set SYM_PIN_152=1")
+def test_reference_grid_152_one_step():
+    """The reference as written: its 152^3 grid and 12 particles, main's
+    set-up and one step, every call equal to the oracle bit for bit."""
+    r = Run(FULL)
+    for where, bad in r.log:
+        assert bad == {}, (where, bad)
 
 
 def test_reference_constants_reproduced():
