@@ -633,13 +633,15 @@ class Parser:
 
 
 def _offset(lo: str) -> str:
+    """Index offset for a lower bound; only integer literals are supported
+    (a unit with another form is reported untranslated)."""
     lo = lo.strip()
     if lo == "0":
         return ""
     if re.fullmatch(r"-?\d+", lo):
         v = int(lo)
         return f"-{v}" if v > 0 else f"+{-v}"
-    return f"-({lo})"
+    raise SyntaxError(f"lower bound {lo!r} is not an integer literal")
 
 
 def parse_expr(s: str, ctx: Ctx) -> Ex:
