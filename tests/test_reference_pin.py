@@ -129,7 +129,7 @@ def test_particles_stay_in_the_domain(run):
         assert int(((V["walls_old"] >= 1) & (V["walls_all"] == 0)).sum()) > 0
 
 
-@pytest.mark.skipif(not os.environ.get("SYM_PIN_152"), reason="about an hour as Python; set SYM_PIN_152=1")
+@pytest.mark.skipif(not os.environ.get("SYM_PIN_152"), reason="about 45 minutes as Python; set SYM_PIN_152=1")
 def test_reference_grid_152_one_step():
     """The reference as written: its 152^3 grid and 12 particles, main's
     set-up and one step, every call equal to the oracle bit for bit."""
