@@ -14,9 +14,10 @@ import os
 
 import pytest
 
-from tests.pin_cases import CASES, OracleCase
+from tests.pin_cases import CASES, FULL, OracleCase
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_pin.json")
+GOLD152 = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_pin_152.json")
 
 
 def _gold():
@@ -51,3 +52,25 @@ def test_digests_cover_every_call():
     g = _gold()
     for name, c in CASES.items():
         assert len(g[name]["snapshots"]) == 1 + 15 * c["steps"]
+
+
+@pytest.mark.skipif(not os.path.exists(GOLD152), reason="no digests of the 152^3 run")
+def test_oracle_reproduces_reference_on_its_own_grid():
+    """The reference as written -- 152^3, the 12 particles of initia_center --
+    main's set-up and one step: the oracle's arrays have the reference's
+    digests after the set-up and after the step (after every call with
+    SYM_PIN_EVERY_CALL=1; hashing 2.4 GB per comparison takes a few seconds)."""
+    with open(GOLD152) as f:
+        g = json.load(f)["full"]
+    assert g["case"] == json.loads(json.dumps(FULL))
+    snaps = g["snapshots"]
+    every = bool(os.environ.get("SYM_PIN_EVERY_CALL"))
+    oc = OracleCase(FULL)
+    assert _mismatch(snaps[0], oc.snapshot()) == [], "setup"
+    i = 0
+    for step, k, call in oc.steps():
+        i += 1
+        assert snaps[i]["after"] == f"{step}:{k}:{call}"
+        if every or i == len(snaps) - 1:
+            assert _mismatch(snaps[i], oc.snapshot()) == [], snaps[i]["after"]
+    assert i == len(snaps) - 1
